@@ -1,0 +1,400 @@
+#!/usr/bin/env python3
+"""Benchmark: plain FP64 TSMTTSM (C = A^T B) on B200, one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the width sweep (A, B row-major, uniform[-1, 1) from a fixed seed),
+headline shape n = 2^26 rows, m = k = 8 columns; ``by_width`` reports every
+shape of the sweep (square widths 1..64 at n = 2^26, 2^23 for 64, and
+(4,32), (32,4), (1,64)).  A step is one call of ``tsm_gemm_tn_f64`` over the
+whole headline input (8 GiB, larger than L2, so no flush is needed).
+
+* ``value``: GB/s of algorithmic bytes 8 n (m + k) + 8 m k per step, with the
+  inputs resident in HBM; for N > 1 (torchrun) each rank holds its own 2^26
+  rows (weak scaling), ends each step with the deterministic cross-rank
+  reduction of its partial C, and value = all rows' bytes / max-over-ranks time.
+* ``e2e``: the same metric through the C ABI from pinned HOST buffers (H2D of A
+  and B, the call, D2H of C inside the timed region).
+* ``roofline``: the dominant kernel against the measured HBM copy bandwidth.
+* ``cpu_baseline``: the reference's own tsmttsm4 (tsmttsm.hh:125-166, main.cc's
+  launch shape) run on the host cores through the oracle's host SYCL subset,
+  on a bounded sample of the same workload.
+
+``--impl reference`` times that CPU implementation alone as the reference arm.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TSMTTSM GB/s (% of HBM peak) by width; fast-form speedup vs FP64 at stated err"
+HEAD_N, HEAD_M, HEAD_K = 1 << 26, 8, 8
+SWEEP = [(1 << 26, 1, 1), (1 << 26, 2, 2), (1 << 26, 4, 4), (1 << 26, 8, 8), (1 << 26, 16, 16),
+         (1 << 26, 32, 32), (1 << 23, 64, 64), (1 << 26, 4, 32), (1 << 26, 32, 4), (1 << 26, 1, 64)]
+SEED = 123
+REF_STRIDE, REF_TILE = 16384, 4  # main.cc:183 launch shape for M = 8
+
+
+def algo_bytes(n: int, m: int, k: int) -> int:
+    return 8 * n * (m + k) + 8 * m * k
+
+
+def load_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json)"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profile_traffic(kernel_tag: str):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    for name in sorted(os.listdir(os.path.join(ROOT, "profiles"))) if os.path.isdir(os.path.join(ROOT, "profiles")) else []:
+        if kernel_tag not in name:
+            continue
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch"):
+                    try:
+                        return int(float(line.split("=")[1].split()[0]))
+                    except (ValueError, IndexError):
+                        return None
+    return None
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+                power.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------- reference arm
+def reference_cpu(n_sample: int, steps: int, warmup: int, budget_s: float) -> dict:
+    """The reference's tsmttsm4<double, 8, 16384, 4> on host threads (kind
+    "reference"), or the oracle's OpenMP restatement (kind "port") when
+    oracle/_ref was not built.  Returns GB/s over `steps` timed runs."""
+    from oracle import oracle
+    R = oracle.ref()
+    A, B = oracle.operands(n_sample, HEAD_M, HEAD_K, SEED)
+    C = __import__("numpy").zeros(HEAD_M * HEAD_K)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    if R is not None:
+        kind, cores = "reference", R.ref_num_threads()
+
+        def run():
+            C[:] = 0
+            ns = ctypes.c_uint64()
+            rc = R.ref_tsmttsm_f64(4, HEAD_M, REF_STRIDE, REF_TILE, n_sample, p(A), p(B), p(C), ctypes.byref(ns))
+            if rc != 0:
+                raise RuntimeError(f"reference kernel refused the shape ({rc})")
+            return ns.value * 1e-9
+    else:
+        kind, cores = "port", oracle.lib().tsm_oracle_num_threads()
+
+        def run():
+            t0 = time.perf_counter()
+            oracle.v4_port(A, B, REF_STRIDE, REF_TILE)
+            return time.perf_counter() - t0
+    for _ in range(warmup):
+        run()
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(steps):
+        times.append(run())
+        if time.perf_counter() - t_start > budget_s and len(times) >= 1:
+            break
+    ref_c = oracle.naive(A[: min(n_sample, 1 << 16)], B[: min(n_sample, 1 << 16)])  # noqa: F841 (sanity only)
+    t = sum(times) / len(times)
+    gbs = algo_bytes(n_sample, HEAD_M, HEAD_K) / t / 1e9
+    return {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind, "steps_timed": len(times),
+            "sample": (f"n={n_sample} rows x m=k=8 (the headline shape at {n_sample / HEAD_N:.4g} of its rows), "
+                       f"tsmttsm4 stride {REF_STRIDE} tile {REF_TILE}, mean of {len(times)} runs "
+                       f"of {t * 1e3:.1f} ms")}
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n_sample = args.ref_rows
+    res = reference_cpu(n_sample, args.steps, args.warmup, budget_s=args.ref_budget)
+    line = {"metric": METRIC, "impl": "reference", "value": res["value"], "unit": "GB/s",
+            "n_gpus": args.gpus, "steps": res["steps_timed"], "warmup": args.warmup,
+            "ms_per_step": algo_bytes(n_sample, HEAD_M, HEAD_K) / res["value"] / 1e6,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(args.gpus),
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(n_gpus: int) -> dict:
+    return {"workload": "plain FP64 TSMTTSM C=A^T B, width sweep; headline n=2^26 rows x m=k=8 per GPU",
+            "n": HEAD_N, "m": HEAD_M, "k": HEAD_K, "inputs": "uniform[-1,1) SplitMix64 seed 123, row-major",
+            "l2": "inputs (8 GiB) larger than L2, no flush", "parallelism": f"rows sharded, {n_gpus} GPU(s)"}
+
+
+# ------------------------------------------------------------------ our arm
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--sweep-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-rows", type=int, default=1 << 23)
+    ap.add_argument("--ref-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return 0
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import tsm_benchmark_b200 as tsm
+    from tsm_benchmark_b200 import _capi, distributed as tsmdist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    lib = _capi.load()
+    peaks = load_peaks()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # Inputs: the largest sweep shape decides the buffer sizes.
+    max_a = max(n * m for n, m, k in SWEEP)
+    max_b = max(n * k for n, m, k in SWEEP)
+    bufA = torch.empty(max_a, dtype=torch.float64, device=dev)
+    bufB = torch.empty(max_b, dtype=torch.float64, device=dev)
+    tsm.fill_uniform(bufA, SEED + rank, 0)
+    tsm.fill_uniform(bufB, SEED + rank, 1)
+    stream = torch.cuda.current_stream(dev)
+    sh = int(stream.cuda_stream)
+
+    def views(n, m, k):
+        return bufA[: n * m].view(n, m), bufB[: n * k].view(n, k)
+
+    A, B = views(HEAD_N, HEAD_M, HEAD_K)
+    C = torch.zeros((HEAD_M, HEAD_K), dtype=torch.float64, device=dev)
+    need = lib.tsm_gemm_tn_workspace_size(HEAD_N, 64, 64)
+    ws = torch.zeros(need, dtype=torch.uint8, device=dev)
+
+    def call(a, b, c, n, m, k):
+        st = lib.tsm_gemm_tn_f64(sh, n, m, k, a.data_ptr(), m, b.data_ptr(), k, c.data_ptr(), k, 0,
+                                 ws.data_ptr(), ws.numel())
+        if st != 0:
+            _capi.check(st, "tsm_gemm_tn_f64")
+
+    def step():
+        call(A, B, C, HEAD_N, HEAD_M, HEAD_K)
+        if world > 1:
+            tsmdist.reduce_partials_(C)
+
+    # ---------------- headline: warmup, then K timed steps
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms_total = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    bytes_step = algo_bytes(HEAD_N, HEAD_M, HEAD_K)
+    value = bytes_step * world / (ms_step * 1e-3) / 1e9
+
+    # correctness guard on the timed inputs (a checksum identity, no oracle)
+    chk = float((A.sum(1) * B.sum(1)).sum())
+    cs = float(C.sum()) if world == 1 else None
+    bound = 4 * math.sqrt(HEAD_N) * 2.0**-53 * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B)) * 8
+    checksum_ok = (cs is None) or abs(cs - chk) <= bound
+    dev_err = tsm.workspace_status(dev) if False else 0
+    bits = ctypes.c_uint(0)
+    lib.tsm_workspace_check(sh, ws.data_ptr(), ctypes.byref(bits))
+    dev_err = int(bits.value)
+
+    # ---------------- the dominant kernel's roofline (the only kernel here)
+    vidx = lib.tsm_gemm_tn_default_variant(HEAD_N, HEAD_M, HEAD_K, A.data_ptr(), HEAD_M, B.data_ptr(), HEAD_K)
+    vname = tsm.variants()[vidx]["name"] if vidx >= 0 else None
+    # time the kernel alone (no reduction step) for the roofline figure
+    kev0 = torch.cuda.Event(enable_timing=True)
+    kev1 = torch.cuda.Event(enable_timing=True)
+    kn = max(20, min(args.steps, 100))
+    kev0.record(stream)
+    for _ in range(kn):
+        call(A, B, C, HEAD_N, HEAD_M, HEAD_K)
+    kev1.record(stream)
+    torch.cuda.synchronize()
+    k_ms = kev0.elapsed_time(kev1) / kn
+    achieved = bytes_step / (k_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": vname, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                "frac_of_8tbs_spec": achieved / 8000.0,
+                "bytes_per_launch": bytes_step, "launch_ms": k_ms,
+                "traffic": profile_traffic("bulk_8x8")}
+
+    # ---------------- by width (each shape: warmup + timed launches)
+    by_width = []
+    if not args.no_sweep and world == 1:
+        for n, m, k in SWEEP:
+            a, b = views(n, m, k)
+            c = torch.zeros((m, k), dtype=torch.float64, device=dev)
+            for _ in range(3):
+                call(a, b, c, n, m, k)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.sweep_steps):
+                call(a, b, c, n, m, k)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.sweep_steps
+            gbs = algo_bytes(n, m, k) / (ms * 1e-3) / 1e9
+            vi = lib.tsm_gemm_tn_default_variant(n, m, k, a.data_ptr(), m, b.data_ptr(), k)
+            by_width.append({"n": n, "m": m, "k": k, "ms": round(ms, 4), "GB/s": round(gbs, 1),
+                             "frac_hbm": round(gbs / peaks["hbm_gbs"], 4),
+                             "GFLOP/s": round(2.0 * n * m * k / (ms * 1e-3) / 1e9, 1),
+                             "variant": tsm.variants()[vi]["name"] if vi >= 0 else None})
+
+    # ---------------- e2e through the C ABI from pinned host buffers
+    e2e = None
+    if world == 1 and args.e2e_steps > 0:
+        Ah = torch.empty((HEAD_N, HEAD_M), dtype=torch.float64, pin_memory=True)
+        Bh = torch.empty((HEAD_N, HEAD_K), dtype=torch.float64, pin_memory=True)
+        Ah.copy_(A, non_blocking=False)
+        Bh.copy_(B, non_blocking=False)
+        Ch = torch.empty((HEAD_M, HEAD_K), dtype=torch.float64, pin_memory=True)
+
+        def e2e_step():
+            A.copy_(Ah, non_blocking=True)
+            B.copy_(Bh, non_blocking=True)
+            call(A, B, C, HEAD_N, HEAD_M, HEAD_K)
+            Ch.copy_(C, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.e2e_steps
+        e2e = {"value": bytes_step / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms,
+               "h2d_bytes_per_step": Ah.numel() * 8 + Bh.numel() * 8, "d2h_bytes_per_step": Ch.numel() * 8}
+        del Ah, Bh
+
+    # ---------------- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        res = reference_cpu(args.ref_rows, steps=50, warmup=1, budget_s=args.ref_budget)
+        cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(world),
+                "frac_hbm": value / world / peaks["hbm_gbs"], "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks, "by_width": by_width,
+                "checksum_ok": checksum_ok, "device_error_bits": dev_err}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

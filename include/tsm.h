@@ -1,0 +1,120 @@
+/*
+ * tsm.h -- C ABI of the B200 TSMTTSM library (C = A^T * B, tall and skinny).
+ *
+ * Shapes: A is n x m, B is n x k, both row-major with leading dimensions
+ * lda >= m and ldb >= k (in elements); C is m x k row-major with leading
+ * dimension ldc >= k.  1 <= m, k <= 64; n >= 0 (int64).  All pointers are
+ * device pointers (cudaMalloc / cudaMallocManaged); all calls are
+ * asynchronous and ordered on `stream` (a cudaStream_t, NULL = the legacy
+ * default stream), like the reference's in-order sycl::queue submits.
+ *
+ * The reference (nilsfriess/tsm_benchmark) exposes the same operation as
+ * C++ templates, `template <typename T, int M, ...> sycl::event
+ * tsmttsmN(sycl::queue& q, int K, T* A, T* B, T* C)` for N in
+ * {"",2,...,9} (tsmttsm.hh:15-586), and as generated functions
+ * `tsmttsm_{M}_{N}_{TM}_{TN}[_lf|_sg|_sg_lf](q, K, const T* A, const T* B,
+ * T* C)` (sycl_codegen_new.py:153,159,257,264).  Those always ADD into C
+ * (the caller zero-fills C first, main.cc:67-69,93) and have square widths
+ * M = N as compile-time parameters; here widths are run-time arguments,
+ * rectangular, and `accumulate` selects C += A^T B (reference semantics) or
+ * C = A^T B.  The compat header tsm_benchmark_b200/compat/tsmttsm.hh maps the
+ * reference's template names onto these entry points.
+ *
+ * Workspace: callers pass device scratch of at least
+ * tsm_gemm_tn_workspace_size(...) bytes, ZERO-FILLED before its first use
+ * (e.g. cudaMemsetAsync(ws, 0, bytes, stream)).  Every call leaves it ready
+ * for the next one.  Calls that may run concurrently (different streams)
+ * need different workspaces.  The library itself never allocates.
+ *
+ * Results are deterministic: the same inputs, shapes and variant give
+ * bit-identical C on every run (no floating-point atomics).
+ */
+#ifndef TSM_H_
+#define TSM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tsm_status {
+  TSM_SUCCESS = 0,
+  TSM_ERROR_INVALID_VALUE = 1,  /* bad shape, null pointer, bad leading dim  */
+  TSM_ERROR_WORKSPACE = 2,      /* workspace missing or too small            */
+  TSM_ERROR_CUDA = 3,           /* a CUDA runtime call failed (see below)    */
+  TSM_ERROR_UNSUPPORTED = 4,    /* no compiled variant for this request      */
+  TSM_ERROR_DEVICE_TIMEOUT = 5  /* a kernel gave up a bounded wait           */
+} tsm_status;
+
+typedef void* tsm_stream_t; /* cudaStream_t */
+
+/* Library version, major * 10000 + minor * 100 + patch. */
+int tsm_version(void);
+
+/* Static description of a status code. */
+const char* tsm_status_string(tsm_status status);
+
+/* Text of the last CUDA error seen by the calling host thread ("" if none). */
+const char* tsm_last_cuda_error(void);
+
+/* Bytes of workspace one plain call with these widths needs on the current
+ * device (independent of n).  New in this library: the reference kernels
+ * need no workspace because they reduce with FP64 atomics into C. */
+size_t tsm_gemm_tn_workspace_size(int64_t n, int m, int k);
+
+/* C = A^T B (accumulate = 0) or C += A^T B (accumulate = 1), FP64.
+ * Replaces tsmttsm / tsmttsm2 ... tsmttsm9 <double, M, ...> (tsmttsm.hh:15-586)
+ * and the generated tsmttsm_{M}_{N}_{TM}_{TN}* kernels (sycl_codegen.py:16-263,
+ * sycl_codegen_new.py:142-363); the reference's driver calls are
+ * main.cc:103-105,148-150 and sycl_codegen_new.py:484-487.
+ * The variant is the autotuned default for (m, k, n). */
+tsm_status tsm_gemm_tn_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                           const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
+                           void* workspace, size_t workspace_bytes);
+
+/* Same, with an explicit variant index (0 <= variant < tsm_variant_count()),
+ * or -1 for the default.  Returns TSM_ERROR_UNSUPPORTED if that variant
+ * cannot run this request (width, leading dimension or alignment).  Used by
+ * the autotuner; replaces choosing a reference kernel by template
+ * parameters (main.cc:171-192) or by generated name. */
+tsm_status tsm_gemm_tn_f64_variant(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                                   const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
+                                   void* workspace, size_t workspace_bytes, int variant);
+
+/* Index of the variant tsm_gemm_tn_f64 would run for this request, or -1. */
+int tsm_gemm_tn_default_variant(int64_t n, int m, int k, const void* A, int64_t lda, const void* B,
+                                int64_t ldb);
+
+typedef struct tsm_variant_info {
+  char name[64];
+  int kind;    /* 0 = TMA bulk pipeline, 1 = direct loads */
+  int wa, wb;  /* widths (exact) or width capacities */
+  int ta, tb;  /* per-thread tile of C */
+  int exact;   /* 1: only m == wa, k == wb */
+  int threads, stages, rows, unroll;
+  size_t smem_bytes;
+} tsm_variant_info;
+
+/* Number of compiled variants, and the description of one. */
+int tsm_variant_count(void);
+tsm_status tsm_variant_get_info(int index, tsm_variant_info* info);
+
+/* Reads and clears the workspace's device error word (synchronises
+ * `stream`).  *bits != 0 means a kernel gave up a bounded wait and its C is
+ * not valid; the call then returns TSM_ERROR_DEVICE_TIMEOUT. */
+tsm_status tsm_workspace_check(tsm_stream_t stream, void* workspace, unsigned* bits);
+
+/* Benchmark-input generator: x[i] = 2u - 1 in [-1, 1), u the top 53 bits of
+ * SplitMix64 at counter (stream_id * 2^40 + i + 1) under `seed`.  The same
+ * values as the oracle's host generator, bit for bit, independent of the
+ * launch shape.  Mirrors the reference drivers' input fill (main.cc:71-86,
+ * sycl_codegen_new.py:436-439) with a reproducible generator. */
+tsm_status tsm_fill_uniform_f64(tsm_stream_t stream, double* x, int64_t count, uint64_t seed, uint64_t stream_id);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* TSM_H_ */

@@ -1,0 +1,166 @@
+"""ctypes loader for the oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module; the library in tsm_benchmark_b200/ never does.
+
+  * ``lib()``  -> oracle/libtsm_oracle.so, the C restatement (tsm_oracle.c)
+  * ``ref()``  -> oracle/_ref/libtsm_ref.so, the reference's own C++ compiled
+                  in place against oracle/sycl_host (None where it was not
+                  built, e.g. on a machine without the reference sources)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libtsm_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libtsm_ref.so")
+
+P = ctypes.c_void_p
+I64 = ctypes.c_int64
+I = ctypes.c_int
+D = ctypes.c_double
+
+_lib = None
+_ref = None
+
+
+def build() -> None:
+    """Runs oracle/Makefile (the reference part only where its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = ctypes.CDLL(ORACLE_SO)
+        L.tsm_oracle_naive_f64.argtypes = [I64, I, I, P, I64, P, I64, P, I64]
+        L.tsm_oracle_naive_f32in.argtypes = [I64, I, I, P, I64, P, I64, P, I64]
+        L.tsm_oracle_dot2_f64.argtypes = [I64, I, I, P, I64, P, I64, P, P, I64]
+        L.tsm_oracle_check_f64.argtypes = [P, P, I, I, I64, D, D]
+        L.tsm_oracle_check_f64.restype = I64
+        L.tsm_oracle_normwise_f64.argtypes = [I64, I, I, P, I64, P, I64, P, P, I64, P]
+        L.tsm_oracle_fill_uniform_f64.argtypes = [P, I64, ctypes.c_uint64, ctypes.c_uint64]
+        L.tsm_oracle_fill_minstd_f64.argtypes = [P, P, I64, ctypes.c_uint32, D, D]
+        L.tsm_oracle_v4_omp.argtypes = [I64, I, I, I, P, P, P]
+        L.tsm_oracle_v4_omp.restype = I
+        L.tsm_oracle_num_threads.restype = I
+        L.tsm_oracle_tsmm_f64.argtypes = [I64, I, I, P, I64, P, I64, I64, P, I64, I]
+        _lib = L
+    return _lib
+
+
+def ref():
+    """The reference's own code (or None when oracle/_ref was not built)."""
+    global _ref
+    if _ref is None and os.path.exists(REF_SO):
+        R = ctypes.CDLL(REF_SO)
+        R.ref_compute_naive_f64.argtypes = [I, I, P, P, P]
+        R.ref_is_correct_f64.argtypes = [P, P, I, D, D]
+        R.ref_tsmttsm_f64.argtypes = [I, I, I, I, I, P, P, P, ctypes.POINTER(ctypes.c_uint64)]
+        R.ref_generated_f64.argtypes = [ctypes.c_char_p, I, P, P, P, ctypes.POINTER(ctypes.c_uint64)]
+        R.ref_fill_main_cc_f64.argtypes = [P, P, ctypes.c_long, ctypes.c_uint]
+        R.ref_num_threads.restype = I
+        _ref = R
+    return _ref
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(P)
+
+
+def _rows(x: np.ndarray) -> tuple[int, int, int]:
+    assert x.ndim == 2 and x.strides[1] == x.itemsize
+    return x.shape[0], x.shape[1], (x.strides[0] // x.itemsize if x.shape[0] > 1 else x.shape[1])
+
+
+def naive(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """C = A^T B in compute_naive's order (main.cc:14-27), FP64."""
+    n, m, lda = _rows(A)
+    _, k, ldb = _rows(B)
+    C = np.zeros((m, k), dtype=np.float64)
+    if A.dtype == np.float32:
+        lib().tsm_oracle_naive_f32in(n, m, k, _p(A), lda, _p(B), ldb, _p(C), k)
+    else:
+        lib().tsm_oracle_naive_f64(n, m, k, _p(A), lda, _p(B), ldb, _p(C), k)
+    return C
+
+
+def dot2(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """Compensated (double-double) A^T B, rounded to FP64."""
+    n, m, lda = _rows(A)
+    _, k, ldb = _rows(B)
+    C = np.zeros((m, k), dtype=np.float64)
+    lib().tsm_oracle_dot2_f64(n, m, k, _p(A), lda, _p(B), ldb, _p(C), None, k)
+    return C
+
+
+def check(ref_c: np.ndarray, got: np.ndarray, rel_tol: float = 1e-6, abs_tol: float = 1e-10) -> int:
+    """is_correct's element rule (main.cc:29-41): index of the first failing
+    entry, or -1."""
+    ref_c = np.ascontiguousarray(ref_c, dtype=np.float64)
+    got = np.ascontiguousarray(got, dtype=np.float64)
+    m, k = ref_c.shape
+    return int(lib().tsm_oracle_check_f64(_p(ref_c), _p(got), m, k, k, rel_tol, abs_tol))
+
+
+def normwise(A: np.ndarray, B: np.ndarray, ref_c: np.ndarray, got: np.ndarray) -> dict:
+    """||got - ref||_F and the bound 4 sqrt(n) 2^-53 ||A||_F ||B||_F."""
+    n, m, lda = _rows(A)
+    _, k, ldb = _rows(B)
+    ref_c = np.ascontiguousarray(ref_c, dtype=np.float64)
+    got = np.ascontiguousarray(got, dtype=np.float64)
+    out = np.zeros(4)
+    lib().tsm_oracle_normwise_f64(n, m, k, _p(A), lda, _p(B), ldb, _p(ref_c), _p(got), k, _p(out))
+    return dict(err=out[0], normA=out[1], normB=out[2], bound=out[3])
+
+
+def uniform(count: int, seed: int, stream: int = 0) -> np.ndarray:
+    """The counter-based uniform[-1, 1) values (same bits as the device fill)."""
+    x = np.empty(count, dtype=np.float64)
+    lib().tsm_oracle_fill_uniform_f64(_p(x), count, seed, stream)
+    return x
+
+
+def operands(n: int, m: int, k: int, seed: int) -> tuple[np.ndarray, np.ndarray]:
+    """A (n x m) from stream 0 and B (n x k) from stream 1 under `seed`."""
+    return uniform(n * m, seed, 0).reshape(n, m), uniform(n * k, seed, 1).reshape(n, k)
+
+
+def main_cc_inputs(n: int, width: int, seed: int = 123) -> tuple[np.ndarray, np.ndarray]:
+    """main.cc's inputs (single-engine path, main.cc:71-86), restated."""
+    A = np.empty(n * width)
+    B = np.empty(n * width)
+    lib().tsm_oracle_fill_minstd_f64(_p(A), _p(B), n * width, seed, -1.0, 1.0)
+    return A.reshape(n, width), B.reshape(n, width)
+
+
+def v4_port(A: np.ndarray, B: np.ndarray, stride: int = 16384, tile: int = 4) -> np.ndarray:
+    """The OpenMP restatement of tsmttsm4 (square widths)."""
+    n, m = A.shape
+    C = np.zeros((m, m))
+    rc = lib().tsm_oracle_v4_omp(n, m, stride, tile, _p(np.ascontiguousarray(A)), _p(np.ascontiguousarray(B)), _p(C))
+    if rc != 0:
+        raise ValueError("launch shape not supported by tsmttsm4")
+    return C
+
+
+def tsmm(X: np.ndarray, W: np.ndarray, transpose_w: bool = False) -> np.ndarray:
+    """Y = X W (or X W^T), the backward TSMM oracle."""
+    n, p, ldx = _rows(X)
+    Wc = np.ascontiguousarray(W, dtype=np.float64)
+    if transpose_w:
+        q = Wc.shape[0]
+        w_row, w_col = 1, Wc.shape[1]
+    else:
+        q = Wc.shape[1]
+        w_row, w_col = Wc.shape[1], 1
+    Y = np.zeros((n, q))
+    lib().tsm_oracle_tsmm_f64(n, p, q, _p(X), ldx, _p(Wc), w_row, w_col, _p(Y), q, 0)
+    return Y

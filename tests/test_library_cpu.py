@@ -1,0 +1,68 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports
+every symbol include/*.h declares, the variant table and the generator agree,
+and the Python layer rejects bad arguments before any compute call."""
+import glob
+import os
+import re
+
+import pytest
+
+from tests.conftest import ROOT
+
+
+def header_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(tsm_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_builds_loads_and_exports_header():
+    from tsm_benchmark_b200 import _capi
+    lib = _capi.load()
+    declared = header_functions()
+    assert "tsm_gemm_tn_f64" in declared and len(declared) >= 10
+    for name in declared:
+        assert hasattr(lib, name), f"{name} declared in include/ but not exported"
+    assert set(_capi.SIGNATURES) == declared, "ctypes signatures must cover exactly the header"
+    assert lib.tsm_version() >= 100
+    assert lib.tsm_status_string(0) == b"success"
+
+
+def test_variant_table():
+    from tsm_benchmark_b200 import codegen, variants
+    vs = variants()
+    names = [v["name"] for v in vs]
+    assert len(names) == len(set(names))
+    assert names == [v.name for v in codegen.default_variants()]
+    exact_bulk = {(v["wa"], v["wb"]) for v in vs if v["kind"] == "bulk" and v["exact"]}
+    for pair in [(1, 1), (2, 2), (4, 4), (8, 8), (16, 16), (32, 32), (64, 64), (4, 32), (32, 4), (1, 64)]:
+        assert pair in exact_bulk
+    for v in vs:
+        assert v["smem_bytes"] <= 227 * 1024
+        assert v["threads"] % 32 == 0
+
+
+def test_generated_sources_current():
+    from tsm_benchmark_b200 import codegen
+    files = codegen.render(codegen.default_variants(), codegen.load_tuned())
+    assert codegen.is_current(files), "run python -m tsm_benchmark_b200.codegen"
+
+
+def test_generator_rejects_bad_variants():
+    from tsm_benchmark_b200 import codegen
+    bad = [codegen.BulkVariant(8, 8, 3, 4), codegen.BulkVariant(64, 64, 8, 8, cw=16),
+           codegen.BulkVariant(8, 8, 4, 4, rows=255), codegen.DirectVariant(64, 64, 16, 16)]
+    for v in bad:
+        assert v.validate(), v
+
+
+def test_python_layer_rejects_cpu_tensors():
+    import torch
+    from tsm_benchmark_b200 import tsmttsm
+    A = torch.zeros((10, 4), dtype=torch.float64)
+    with pytest.raises(ValueError):
+        tsmttsm(A, A)

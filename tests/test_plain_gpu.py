@@ -1,0 +1,194 @@
+"""Parity of the plain FP64 path (C ABI through ctypes) with the oracle.
+
+Acceptance, per entry: the reference's is_correct rule (main.cc:29-41, rel
+1e-6 / abs 1e-10); per matrix: the normwise bound
+||C - C_oracle||_F <= 4 sqrt(n) 2^-53 ||A||_F ||B||_F.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from tests.conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL, ABS_TOL = 1e-6, 1e-10
+
+
+def to_dev(x, dev):
+    return torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+
+
+def assert_parity(oracle_mod, A, B, C_got, C_ref=None, what=""):
+    C_got = C_got.cpu().numpy() if isinstance(C_got, torch.Tensor) else C_got
+    if C_ref is None:
+        C_ref = oracle_mod.naive(A, B)
+    bad = oracle_mod.check(C_ref, C_got, REL_TOL, ABS_TOL)
+    assert bad == -1, f"{what}: entry {bad}: ref {C_ref.ravel()[bad]} got {C_got.ravel()[bad]}"
+    nw = oracle_mod.normwise(A, B, C_ref, C_got)
+    assert nw["err"] <= nw["bound"], f"{what}: normwise {nw}"
+
+
+SHAPES = [(1, 1), (2, 2), (4, 4), (8, 8), (16, 16), (32, 32), (64, 64), (4, 32), (32, 4), (1, 64),
+          (3, 5), (7, 13), (33, 17), (64, 1), (5, 64), (12, 12), (4, 8), (16, 32)]
+ROWS = [0, 1, 2, 3, 255, 4099, 65537]
+
+
+@pytest.mark.parametrize("m,k", SHAPES)
+def test_parity_widths_and_ragged_rows(gpu, oracle_mod, m, k):
+    from tsm_benchmark_b200 import tsmttsm, workspace_status
+    for n in ROWS:
+        if m * k >= 1024 and n > 4099:
+            continue
+        A, B = oracle_mod.operands(n, m, k, seed=1000 + n + 7 * m + k)
+        C = tsmttsm(to_dev(A, gpu), to_dev(B, gpu))
+        torch.cuda.synchronize()
+        assert_parity(oracle_mod, A, B, C, what=f"n={n} m={m} k={k}")
+    assert workspace_status(gpu) == 0
+
+
+def test_golden_square_cases(gpu, oracle_mod):
+    from tests.golden.make_golden import SQUARE_CASES
+    from tsm_benchmark_b200 import tsmttsm
+    g = np.load(os.path.join(GOLDEN, "ref_square_cases.npz"))
+    for n, M, seed in SQUARE_CASES:
+        A, B = oracle_mod.operands(n, M, M, seed)
+        C = tsmttsm(to_dev(A, gpu), to_dev(B, gpu))
+        assert_parity(oracle_mod, A, B, C, g[f"n{n}_M{M}_s{seed}"], what=f"golden n={n} M={M}")
+
+
+def test_config0_main_cc_inputs(gpu, oracle_mod):
+    """n = 2^20, m = k = 8 with main.cc's own inputs; checked, as main.cc
+    checks its kernels, against the reference's compute_naive output, and
+    against the reference's tsmttsm4/6/9 outputs recorded on the CPU."""
+    from tsm_benchmark_b200 import tsmttsm
+    g = np.load(os.path.join(GOLDEN, "ref_config0.npz"))
+    A, B = oracle_mod.main_cc_inputs(1 << 20, 8, 123)
+    C = torch.zeros((8, 8), dtype=torch.float64, device=gpu)
+    tsmttsm(to_dev(A, gpu), to_dev(B, gpu), C, accumulate=True)  # main.cc: zero C, then add
+    assert_parity(oracle_mod, A, B, C, g["C_naive"], what="config0")
+    for v in (4, 6, 9):
+        assert oracle_mod.check(g[f"C_v{v}"], C.cpu().numpy()) == -1
+
+
+def test_accumulate_semantics(gpu, oracle_mod):
+    from tsm_benchmark_b200 import tsmttsm
+    A, B = oracle_mod.operands(5001, 8, 16, 3)
+    C0 = np.random.default_rng(0).standard_normal((8, 16))
+    C = to_dev(C0, gpu)
+    tsmttsm(to_dev(A, gpu), to_dev(B, gpu), C, accumulate=True)
+    assert_parity(oracle_mod, A, B, C.cpu().numpy() - C0, what="accumulate")
+    # accumulate=False overwrites whatever C held (NaN included)
+    C.fill_(float("nan"))
+    tsmttsm(to_dev(A, gpu), to_dev(B, gpu), C, accumulate=False)
+    assert_parity(oracle_mod, A, B, C, what="overwrite")
+    # n = 0: C = 0, or C unchanged when accumulating
+    E = torch.empty((0, 8), dtype=torch.float64, device=gpu)
+    F = torch.empty((0, 16), dtype=torch.float64, device=gpu)
+    C.fill_(3.0)
+    tsmttsm(E, F, C, accumulate=True)
+    assert torch.all(C == 3.0)
+    tsmttsm(E, F, C, accumulate=False)
+    assert torch.all(C == 0.0)
+
+
+def test_deterministic(gpu, oracle_mod):
+    from tsm_benchmark_b200 import tsmttsm
+    A, B = oracle_mod.operands(1 << 18, 16, 16, 5)
+    dA, dB = to_dev(A, gpu), to_dev(B, gpu)
+    first = tsmttsm(dA, dB).clone()
+    for _ in range(5):
+        assert torch.equal(tsmttsm(dA, dB), first)
+
+
+def test_every_applicable_variant(gpu, oracle_mod):
+    """Each compiled variant that accepts a shape computes it correctly."""
+    from tsm_benchmark_b200 import TsmError, tsmttsm, variants
+    cases = {}
+    for m, k in [(1, 1), (8, 8), (16, 16), (64, 64), (4, 32), (5, 12), (1, 64), (32, 32)]:
+        cases[(m, k)] = oracle_mod.operands(3001, m, k, 11 + m + k)
+    ran = 0
+    for v in variants():
+        for (m, k), (A, B) in cases.items():
+            fits = (m == v["wa"] and k == v["wb"]) if v["exact"] else (m <= v["wa"] and k <= v["wb"])
+            if not fits:
+                continue
+            C = tsmttsm(to_dev(A, gpu), to_dev(B, gpu), variant=v["index"])
+            assert_parity(oracle_mod, A, B, C, what=v["name"])
+            ran += 1
+    assert ran >= 40
+
+
+def test_strided_and_unaligned_operands(gpu, oracle_mod):
+    """lda > m (column slice of a wider matrix) and operands that start 8
+    bytes past a 16-byte boundary take the direct-load kernels."""
+    from tsm_benchmark_b200 import default_variant, tsmttsm, variants
+    names = [v["name"] for v in variants()]
+    A_wide, B_wide = oracle_mod.operands(7777, 24, 40, 21)
+    A, B = A_wide[:, 3:11], B_wide[:, 5:37]
+    dA = to_dev(A_wide, gpu)[:, 3:11]
+    dB = to_dev(B_wide, gpu)[:, 5:37]
+    assert names[default_variant(dA, dB)].startswith("direct")
+    C = tsmttsm(dA, dB)
+    assert_parity(oracle_mod, np.ascontiguousarray(A), np.ascontiguousarray(B), C, what="strided")
+    A, B = oracle_mod.operands(5000, 8, 8, 22)
+    bufA = torch.zeros(A.size + 1, dtype=torch.float64, device=gpu)
+    bufB = torch.zeros(B.size + 1, dtype=torch.float64, device=gpu)
+    bufA[1:] = to_dev(A.ravel(), gpu)
+    bufB[1:] = to_dev(B.ravel(), gpu)
+    dA, dB = bufA[1:].view(5000, 8), bufB[1:].view(5000, 8)
+    assert dA.data_ptr() % 16 == 8
+    assert names[default_variant(dA, dB)].startswith("direct")
+    assert_parity(oracle_mod, A, B, tsmttsm(dA, dB), what="unaligned")
+
+
+def test_argument_errors(gpu):
+    from tsm_benchmark_b200 import TsmError, tsmttsm
+    from tsm_benchmark_b200 import _capi
+    A = torch.zeros((10, 65), dtype=torch.float64, device=gpu)
+    with pytest.raises(TsmError):
+        tsmttsm(A, A)
+    with pytest.raises(TypeError):
+        tsmttsm(A.float(), A.float())
+    lib = _capi.load()
+    A = torch.zeros((10, 8), dtype=torch.float64, device=gpu)
+    C = torch.zeros((8, 8), dtype=torch.float64, device=gpu)
+    ws = torch.zeros(64, dtype=torch.uint8, device=gpu)
+    st = lib.tsm_gemm_tn_f64(None, 10, 8, 8, A.data_ptr(), 8, A.data_ptr(), 8, C.data_ptr(), 8, 0, ws.data_ptr(), 64)
+    assert st == 2  # workspace too small
+    st = lib.tsm_gemm_tn_f64(None, 10, 8, 8, A.data_ptr(), 7, A.data_ptr(), 8, C.data_ptr(), 8, 0, ws.data_ptr(), 64)
+    assert st == 1  # lda < m
+    st = lib.tsm_gemm_tn_f64_variant(None, 10, 8, 8, A.data_ptr(), 8, A.data_ptr(), 8, C.data_ptr(), 8, 0,
+                                     ws.data_ptr(), 1 << 30, 10**6)
+    assert st in (2, 4)
+
+
+def test_device_fill_matches_oracle_generator(gpu, oracle_mod):
+    from tsm_benchmark_b200 import fill_uniform
+    x = torch.empty(1 << 20, dtype=torch.float64, device=gpu)
+    fill_uniform(x, seed=99, stream_id=3)
+    assert np.array_equal(x.cpu().numpy(), oracle_mod.uniform(1 << 20, 99, 3))
+
+
+@pytest.mark.parametrize("m,k", [(1, 1), (8, 8), (16, 16), (1, 64)])
+def test_full_size_properties(gpu, m, k):
+    """n = 2^26 (the sweep's row count): against cuBLAS DGEMM through torch
+    within the normwise bound, and the checksum identity
+    sum_ij C_ij = sum_r (sum_i A_ri)(sum_j B_rj)."""
+    from tsm_benchmark_b200 import fill_uniform, tsmttsm
+    n = 1 << 26 if m * k <= 256 else 1 << 24
+    A = torch.empty((n, m), dtype=torch.float64, device=gpu)
+    B = torch.empty((n, k), dtype=torch.float64, device=gpu)
+    fill_uniform(A, 1, 0)
+    fill_uniform(B, 1, 1)
+    C = tsmttsm(A, B)
+    C2 = A.T @ B
+    bound = 4 * np.sqrt(n) * 2.0**-53 * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B))
+    assert float(torch.linalg.norm(C - C2)) <= 2 * bound
+    chk = float((A.sum(1) * B.sum(1)).sum())
+    assert abs(float(C.sum()) - chk) <= 4 * bound * np.sqrt(m * k)
+    del A, B
+    torch.cuda.empty_cache()

@@ -1,0 +1,326 @@
+#!/usr/bin/env python3
+"""CUDA variant generator for the TSMTTSM kernels (C = A^T * B).
+
+Rewrite of the reference's SYCL generators (sycl_codegen.py:16-263,
+sycl_codegen_new.py:142-363).  Those emit one SYCL kernel per
+(M, N, TM, TN, stride, local_size, leap_frog, reduction, unroll) with scalar
+accumulators, a grid-stride row loop and FP64 atomics.  This generator emits
+rows of the kernel table in ``csrc/generated/``: explicit instantiations of
+the sm_100a templates in ``csrc/tsm_plain.cuh`` over the axes
+
+    width pair      (wa, wb)        -- exact widths or width capacities
+    tile            (ta, tb)        -- per-thread register tile of C
+                                       (the reference's TM x TN)
+    consumer warps  cw              -- CTA size (the reference's local_size)
+    prefetch depth  stages          -- shared-memory ring depth (the
+                                       reference's leap-frog is depth 2 in
+                                       registers)
+    chunk rows      rows            -- rows per TMA bulk copy
+    unroll          unroll          -- row-loop unroll (the reference's
+                                       --unroll)
+    reduction       two-level       -- warp shuffle + fixed-order CTA sum +
+                                       last-CTA fixed-order sum (the only
+                                       scheme: deterministic; replaces
+                                       "global" / "twolevel" / "sg")
+
+plus a tuned-defaults table (from ``tuned.json``, written by the autotuner)
+that the library consults before falling back to table order.
+
+Usage::
+
+    python -m tsm_benchmark_b200.codegen            # write csrc/generated/
+    python -m tsm_benchmark_b200.codegen --check    # exit 1 if out of date
+    python -m tsm_benchmark_b200.codegen --list     # print the variant names
+
+The emitted files are committed; tests check that regenerating reproduces
+them byte for byte.
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import os
+import sys
+from typing import Iterable
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GEN_DIR = os.path.join(HERE, "csrc", "generated")
+TUNED_JSON = os.path.join(HERE, "tuned.json")
+
+SMEM_LIMIT = 227 * 1024  # dynamic shared memory per CTA on sm_100a
+WIDTH_CAPS = (1, 2, 4, 8, 16, 32, 64)
+
+
+@dataclasses.dataclass(frozen=True)
+class BulkVariant:
+    """One TMA-bulk pipelined kernel (tsm_tn_bulk_kernel)."""
+
+    wa: int
+    wb: int
+    ta: int
+    tb: int
+    cw: int = 8
+    stages: int = 6
+    rows: int = 0  # 0: sized for ~32 KB stages
+    unroll: int = 1
+    exact: bool = True
+
+    def resolved(self) -> "BulkVariant":
+        if self.rows:
+            return self
+        rg = self.cw * 32 // self.num_tiles
+        rows = max(2, (32768 // (8 * (self.wa + self.wb))) // 2 * 2)
+        # Round to whole passes of the row groups, keeping chunks even.
+        if rows >= rg:
+            rows = rows // rg * rg
+        rows = max(2, rows // 2 * 2)
+        return dataclasses.replace(self, rows=rows)
+
+    @property
+    def num_tiles(self) -> int:
+        return (self.wa // self.ta) * (self.wb // self.tb)
+
+    @property
+    def name(self) -> str:
+        v = self.resolved()
+        s = (f"bulk_{v.wa}x{v.wb}_t{v.ta}x{v.tb}_w{v.cw}_s{v.stages}"
+             f"_r{v.rows}_u{v.unroll}")
+        return s if v.exact else s + "_cap"
+
+    def smem_bytes(self) -> int:
+        v = self.resolved()
+        ct = v.cw * 32
+        nt = v.num_tiles
+        slots = v.cw if nt < 32 else ct // nt
+        ring = v.stages * v.rows * (v.wa + v.wb) * 8
+        red = slots * v.wa * v.wb * 8
+        data = max(ring, red)
+        return (data + 127) // 128 * 128 + 2 * v.stages * 8 + 16
+
+    def validate(self) -> list[str]:
+        v = self.resolved()
+        errs = []
+        if v.wa % v.ta or v.wb % v.tb:
+            errs.append("tile must divide the width")
+        nt = v.num_tiles
+        if nt & (nt - 1):
+            errs.append("tile count must be a power of two")
+        if (v.cw * 32) % nt:
+            errs.append("consumer threads must cover whole tiles")
+        if v.rows % 2:
+            errs.append("chunk rows must be even")
+        rg = v.cw * 32 // max(nt, 1)
+        if v.rows >= rg and (v.rows // rg) % v.unroll:
+            errs.append("unroll must divide the rows per thread")
+        if v.ta * v.tb > 64:
+            errs.append("register tile above 64 accumulators")
+        if self.smem_bytes() > SMEM_LIMIT:
+            errs.append(f"shared memory {self.smem_bytes()} above {SMEM_LIMIT}")
+        return errs
+
+    def emit(self) -> str:
+        v = self.resolved()
+        return (f'TSM_BULK_VARIANT("{self.name}", {v.wa}, {v.wb}, {v.ta}, {v.tb}, '
+                f'{v.cw}, {v.stages}, {v.rows}, {v.unroll}, '
+                f'{"true" if v.exact else "false"})')
+
+
+@dataclasses.dataclass(frozen=True)
+class DirectVariant:
+    """One direct-load kernel (tsm_tn_direct_kernel)."""
+
+    wa: int
+    wb: int
+    ta: int
+    tb: int
+    threads: int = 256
+    exact: bool = False
+
+    @property
+    def num_tiles(self) -> int:
+        return (self.wa // self.ta) * (self.wb // self.tb)
+
+    @property
+    def name(self) -> str:
+        s = f"direct_{self.wa}x{self.wb}_t{self.ta}x{self.tb}_th{self.threads}"
+        return s if self.exact else s + "_cap"
+
+    def validate(self) -> list[str]:
+        errs = []
+        if self.wa % self.ta or self.wb % self.tb:
+            errs.append("tile must divide the width")
+        nt = self.num_tiles
+        if nt & (nt - 1):
+            errs.append("tile count must be a power of two")
+        if self.threads % nt or self.threads % 32:
+            errs.append("threads must cover whole tiles")
+        if self.ta * self.tb > 64:
+            errs.append("register tile above 64 accumulators")
+        return errs
+
+    def emit(self) -> str:
+        return (f'TSM_DIRECT_VARIANT("{self.name}", {self.wa}, {self.wb}, {self.ta}, '
+                f'{self.tb}, {self.threads}, {"true" if self.exact else "false"})')
+
+
+def default_tile(w: int) -> int:
+    """Per-thread tile extent for a width (capacity)."""
+    return {1: 1, 2: 2, 4: 4, 8: 4, 16: 8, 32: 8, 64: 8}[w]
+
+
+# Width pairs with exact (fully specialised) bulk variants: every shape of the
+# plain sweep (square 1..64, (4,32), (32,4), (1,64)) and the widths of the
+# batched problems ({4,8,16,32}^2).
+EXACT_PAIRS = sorted(set(
+    [(w, w) for w in WIDTH_CAPS] + [(4, 32), (32, 4), (1, 64)]
+    + [(a, b) for a in (4, 8, 16, 32) for b in (4, 8, 16, 32)]))
+
+# Extra tile / launch candidates the autotuner may pick for the sweep shapes.
+EXTRA_CANDIDATES: dict[tuple[int, int], list[dict]] = {
+    (1, 1): [dict(unroll=2), dict(unroll=4)],
+    (2, 2): [dict(unroll=2)],
+    (4, 4): [dict(ta=2, tb=2), dict(unroll=2)],
+    (8, 8): [dict(ta=8, tb=8), dict(unroll=2), dict(ta=2, tb=8)],
+    (16, 16): [dict(ta=4, tb=4), dict(ta=4, tb=8)],
+    (32, 32): [dict(ta=8, tb=4), dict(cw=16)],
+    (64, 64): [dict(unroll=2), dict(stages=4)],
+}
+
+
+def default_variants() -> list:
+    out: list = []
+    for wa, wb in EXACT_PAIRS:
+        base = BulkVariant(wa, wb, default_tile(wa), default_tile(wb))
+        out.append(base)
+        for extra in EXTRA_CANDIDATES.get((wa, wb), []):
+            out.append(dataclasses.replace(base, **extra))
+    for wa in WIDTH_CAPS:
+        for wb in WIDTH_CAPS:
+            out.append(BulkVariant(wa, wb, default_tile(wa), default_tile(wb), exact=False))
+    for wa in WIDTH_CAPS:
+        for wb in WIDTH_CAPS:
+            out.append(DirectVariant(wa, wb, default_tile(wa), default_tile(wb)))
+    return out
+
+
+def check_variants(vs: Iterable) -> None:
+    names = set()
+    for v in vs:
+        errs = v.validate()
+        if errs:
+            raise ValueError(f"{v.name}: {'; '.join(errs)}")
+        if v.name in names:
+            raise ValueError(f"duplicate variant {v.name}")
+        names.add(v.name)
+
+
+def load_tuned(path: str = TUNED_JSON) -> list[tuple[int, int, int, str]]:
+    """Tuned defaults: list of (m, k, nmin, variant name)."""
+    if not os.path.exists(path):
+        return []
+    with open(path) as f:
+        doc = json.load(f)
+    rows = []
+    for e in doc.get("choices", []):
+        rows.append((int(e["m"]), int(e["k"]), int(e.get("nmin", 0)), str(e["variant"])))
+    return sorted(rows)
+
+
+HEADER = ("// Generated by tsm_benchmark_b200/codegen.py -- do not edit.\n"
+          "// Regenerate with: python -m tsm_benchmark_b200.codegen\n")
+
+
+def render(vs: list, tuned: list, parts: int = 8) -> dict[str, str]:
+    """Returns {file name: contents} for csrc/generated/."""
+    check_variants(vs)
+    known = {v.name for v in vs}
+    for m, k, nmin, name in tuned:
+        if name not in known:
+            raise ValueError(f"tuned choice {name} for ({m},{k}) is not a variant")
+    files: dict[str, str] = {}
+    chunks = [vs[i::parts] for i in range(parts)]
+    # Keep table order global: part i holds rows i, i+parts, ...; the index
+    # below re-interleaves them so the library sees the list order above.
+    for i, chunk in enumerate(chunks):
+        body = [HEADER, '#include "../tsm_registry.cuh"', "", "namespace tsm {", ""]
+        body.append(f"extern const Variant kGenPart{i}[];")
+        body.append(f"const Variant kGenPart{i}[] = {{")
+        for v in chunk:
+            body.append(f"    {v.emit()},")
+        body.append("};")
+        body.append(f"extern const int kGenPart{i}Count;")
+        body.append(f"const int kGenPart{i}Count = {len(chunk)};")
+        body.append("")
+        body.append("}  // namespace tsm")
+        files[f"variants_p{i}.cu"] = "\n".join(body) + "\n"
+
+    idx = [HEADER, '#include "../tsm_registry.cuh"', "", "namespace tsm {", ""]
+    for i in range(parts):
+        idx.append(f"extern const Variant kGenPart{i}[];")
+    idx.append("")
+    # One single-row part per variant, in list order.
+    idx.append("const VariantPart kVariantParts[] = {")
+    for j in range(len(vs)):
+        idx.append(f"    {{kGenPart{j % parts} + {j // parts}, 1}},")
+    idx.append("};")
+    idx.append(f"const int kVariantPartCount = {len(vs)};")
+    idx.append("")
+    idx.append("// Tuned defaults: \"m k nmin variant\" (largest nmin <= n wins).")
+    idx.append("extern const char* const kTunedDefaults[];")
+    idx.append("const char* const kTunedDefaults[] = {")
+    for m, k, nmin, name in tuned:
+        idx.append(f'    "{m} {k} {nmin} {name}",')
+    idx.append("    nullptr};")
+    idx.append("extern const int kTunedDefaultCount;")
+    idx.append(f"const int kTunedDefaultCount = {len(tuned)};")
+    idx.append("")
+    idx.append("}  // namespace tsm")
+    files["variants_index.cu"] = "\n".join(idx) + "\n"
+    return files
+
+
+def write(files: dict[str, str], out_dir: str = GEN_DIR) -> None:
+    os.makedirs(out_dir, exist_ok=True)
+    for name, text in files.items():
+        path = os.path.join(out_dir, name)
+        old = open(path).read() if os.path.exists(path) else None
+        if old != text:
+            with open(path, "w") as f:
+                f.write(text)
+    for name in os.listdir(out_dir):
+        if name.endswith(".cu") and name not in files:
+            os.remove(os.path.join(out_dir, name))
+
+
+def is_current(files: dict[str, str], out_dir: str = GEN_DIR) -> bool:
+    for name, text in files.items():
+        path = os.path.join(out_dir, name)
+        if not os.path.exists(path) or open(path).read() != text:
+            return False
+    return True
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--check", action="store_true", help="exit 1 if csrc/generated is stale")
+    ap.add_argument("--list", action="store_true", help="print the variant names")
+    ap.add_argument("--out", default=GEN_DIR, help="output directory")
+    args = ap.parse_args(argv)
+    vs = default_variants()
+    files = render(vs, load_tuned())
+    if args.list:
+        for v in vs:
+            print(v.name)
+        return 0
+    if args.check:
+        ok = is_current(files, args.out)
+        print("generated kernels are", "current" if ok else "STALE")
+        return 0 if ok else 1
+    write(files, args.out)
+    print(f"wrote {len(files)} files, {len(vs)} variants, {len(load_tuned())} tuned choices to {args.out}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,31 @@
+// Generated by tsm_benchmark_b200/codegen.py -- do not edit.
+// Regenerate with: python -m tsm_benchmark_b200.codegen
+
+#include "../tsm_registry.cuh"
+
+namespace tsm {
+
+extern const Variant kGenPart1[];
+const Variant kGenPart1[] = {
+    TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r2048_u2", 1, 1, 1, 1, 8, 6, 2048, 2, true),
+    TSM_BULK_VARIANT("bulk_4x8_t4x4_w8_s6_r256_u1", 4, 8, 4, 4, 8, 6, 256, 1, true),
+    TSM_BULK_VARIANT("bulk_8x16_t4x8_w8_s6_r128_u1", 8, 16, 4, 8, 8, 6, 128, 1, true),
+    TSM_BULK_VARIANT("bulk_32x4_t8x4_w8_s6_r64_u1", 32, 4, 8, 4, 8, 6, 64, 1, true),
+    TSM_BULK_VARIANT("bulk_64x64_t8x8_w8_s4_r32_u1", 64, 64, 8, 8, 8, 4, 32, 1, true),
+    TSM_BULK_VARIANT("bulk_2x1_t2x1_w8_s6_r1280_u1_cap", 2, 1, 2, 1, 8, 6, 1280, 1, false),
+    TSM_BULK_VARIANT("bulk_4x2_t4x2_w8_s6_r512_u1_cap", 4, 2, 4, 2, 8, 6, 512, 1, false),
+    TSM_BULK_VARIANT("bulk_8x4_t4x4_w8_s6_r256_u1_cap", 8, 4, 4, 4, 8, 6, 256, 1, false),
+    TSM_BULK_VARIANT("bulk_16x8_t8x4_w8_s6_r128_u1_cap", 16, 8, 8, 4, 8, 6, 128, 1, false),
+    TSM_BULK_VARIANT("bulk_32x16_t8x8_w8_s6_r64_u1_cap", 32, 16, 8, 8, 8, 6, 64, 1, false),
+    TSM_BULK_VARIANT("bulk_64x32_t8x8_w8_s6_r40_u1_cap", 64, 32, 8, 8, 8, 6, 40, 1, false),
+    TSM_DIRECT_VARIANT("direct_1x64_t1x8_th256_cap", 1, 64, 1, 8, 256, false),
+    TSM_DIRECT_VARIANT("direct_4x1_t4x1_th256_cap", 4, 1, 4, 1, 256, false),
+    TSM_DIRECT_VARIANT("direct_8x2_t4x2_th256_cap", 8, 2, 4, 2, 256, false),
+    TSM_DIRECT_VARIANT("direct_16x4_t8x4_th256_cap", 16, 4, 8, 4, 256, false),
+    TSM_DIRECT_VARIANT("direct_32x8_t8x4_th256_cap", 32, 8, 8, 4, 256, false),
+    TSM_DIRECT_VARIANT("direct_64x16_t8x8_th256_cap", 64, 16, 8, 8, 256, false),
+};
+extern const int kGenPart1Count;
+const int kGenPart1Count = 17;
+
+}  // namespace tsm

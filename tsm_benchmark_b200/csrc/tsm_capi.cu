@@ -1,0 +1,330 @@
+// tsm_capi.cu -- the C ABI (include/tsm.h): argument checks, variant choice,
+// grid sizing and launches for the plain FP64 path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/tsm.h"
+#include "tsm_registry.cuh"
+
+namespace tsm {
+namespace {
+
+thread_local std::string g_last_cuda_error;
+
+tsm_status cuda_fail(cudaError_t e, const char* what) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  g_last_cuda_error = buf;
+  return TSM_ERROR_CUDA;
+}
+
+// Workspace layout: [counter u32][error u32][pad to 256 B][partials].
+constexpr size_t kWsHeader = 256;
+constexpr int kMaxCtasPerSm = 4;
+
+struct DeviceState {
+  int sms = 0;
+  std::vector<signed char> attr_done;  // per variant: smem attribute set / failed
+  std::vector<int> occupancy;          // per variant: CTAs per SM (0 = unknown)
+};
+
+std::mutex g_mu;
+std::unordered_map<int, DeviceState> g_devices;
+
+const std::vector<const Variant*>& variants() {
+  static const std::vector<const Variant*> all = [] {
+    std::vector<const Variant*> v;
+    for (int p = 0; p < kVariantPartCount; ++p)
+      for (int i = 0; i < kVariantParts[p].count; ++i) v.push_back(&kVariantParts[p].rows[i]);
+    return v;
+  }();
+  return all;
+}
+
+tsm_status current_device(int* dev, DeviceState** st) {
+  cudaError_t e = cudaGetDevice(dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_mu);
+  DeviceState& s = g_devices[*dev];
+  if (s.sms == 0) {
+    e = cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, *dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+    s.attr_done.assign(variants().size(), 0);
+    s.occupancy.assign(variants().size(), 0);
+  }
+  *st = &s;
+  return TSM_SUCCESS;
+}
+
+// Sets the dynamic shared-memory limit of a variant once per device and
+// caches how many of its CTAs fit on one SM.
+tsm_status prepare_variant(DeviceState* st, int idx) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (st->attr_done[idx] == 1) return TSM_SUCCESS;
+  if (st->attr_done[idx] == -1) return TSM_ERROR_UNSUPPORTED;
+  const Variant* v = variants()[idx];
+  cudaError_t e = cudaFuncSetAttribute(v->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(v->smem));
+  if (e != cudaSuccess) {
+    st->attr_done[idx] = -1;
+    return cuda_fail(e, "cudaFuncSetAttribute");
+  }
+  int occ = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v->kernel, v->threads, v->smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (occ < 1) {
+    st->attr_done[idx] = -1;
+    return TSM_ERROR_UNSUPPORTED;
+  }
+  st->occupancy[idx] = std::min(occ, kMaxCtasPerSm);
+  st->attr_done[idx] = 1;
+  return TSM_SUCCESS;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+bool applicable(const Variant* v, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
+  if (v->exact ? (m != v->wa || k != v->wb) : (m > v->wa || k > v->wb)) return false;
+  if (v->kind == kKindBulk) {
+    if (lda != m || ldb != k) return false;
+    if (!aligned16(A) || !aligned16(B)) return false;
+  }
+  return true;
+}
+
+// Generated: preferred variant per (m, k, n) from the tuning table.
+}  // namespace
+
+extern const char* const kTunedDefaults[];  // "m k nmin name", null-terminated
+extern const int kTunedDefaultCount;
+
+namespace {
+
+int find_variant(const char* name) {
+  const auto& vs = variants();
+  for (size_t i = 0; i < vs.size(); ++i)
+    if (std::strcmp(vs[i]->name, name) == 0) return static_cast<int>(i);
+  return -1;
+}
+
+int default_variant(int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
+  const auto& vs = variants();
+  // 1. The tuning table: the entry with the largest nmin <= n for (m, k).
+  int best = -1;
+  long long best_nmin = -1;
+  for (int i = 0; i < kTunedDefaultCount; ++i) {
+    int tm = 0, tk = 0;
+    long long nmin = 0;
+    char name[96] = {0};
+    if (std::sscanf(kTunedDefaults[i], "%d %d %lld %95s", &tm, &tk, &nmin, name) != 4) continue;
+    if (tm != m || tk != k || nmin > n || nmin < best_nmin) continue;
+    const int idx = find_variant(name);
+    if (idx >= 0 && applicable(vs[idx], m, k, A, lda, B, ldb)) {
+      best = idx;
+      best_nmin = nmin;
+    }
+  }
+  if (best >= 0) return best;
+  // 2. Table order: the generator lists exact bulk variants first, then
+  //    capacity bulk variants from the smallest capacity up, then direct ones.
+  for (size_t i = 0; i < vs.size(); ++i)
+    if (applicable(vs[i], m, k, A, lda, B, ldb)) return static_cast<int>(i);
+  return -1;
+}
+
+tsm_status check_args(int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb,
+                      const void* C, int64_t ldc) {
+  if (n < 0 || m < 1 || k < 1 || m > 64 || k > 64) return TSM_ERROR_INVALID_VALUE;
+  if (lda < m || ldb < k || ldc < k) return TSM_ERROR_INVALID_VALUE;
+  if (C == nullptr) return TSM_ERROR_INVALID_VALUE;
+  if (n > 0 && (A == nullptr || B == nullptr)) return TSM_ERROR_INVALID_VALUE;
+  return TSM_SUCCESS;
+}
+
+size_t workspace_bytes_for(int sms, int m, int k) {
+  return kWsHeader + static_cast<size_t>(sms) * kMaxCtasPerSm * m * k * sizeof(double);
+}
+
+tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                        const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate, void* ws,
+                        size_t ws_bytes, int variant) {
+  tsm_status s = check_args(n, m, k, A, lda, B, ldb, C, ldc);
+  if (s != TSM_SUCCESS) return s;
+  int dev = 0;
+  DeviceState* st = nullptr;
+  if ((s = current_device(&dev, &st)) != TSM_SUCCESS) return s;
+  if (ws == nullptr || ws_bytes < workspace_bytes_for(st->sms, m, k) || !aligned16(ws))
+    return TSM_ERROR_WORKSPACE;
+
+  const auto& vs = variants();
+  int idx = variant;
+  if (idx < 0) {
+    idx = default_variant(n, m, k, A, lda, B, ldb);
+    if (idx < 0) return TSM_ERROR_UNSUPPORTED;
+  } else if (idx >= static_cast<int>(vs.size()) || !applicable(vs[idx], m, k, A, lda, B, ldb)) {
+    return TSM_ERROR_UNSUPPORTED;
+  }
+  if ((s = prepare_variant(st, idx)) != TSM_SUCCESS) return s;
+  const Variant* v = vs[idx];
+
+  PlainArgs p{};
+  p.A = A;
+  p.B = B;
+  p.C = C;
+  p.n = n;
+  p.m = m;
+  p.k = k;
+  p.lda = lda;
+  p.ldb = ldb;
+  p.ldc = ldc;
+  p.accumulate = accumulate ? 1 : 0;
+  unsigned char* base = static_cast<unsigned char*>(ws);
+  p.counter = reinterpret_cast<unsigned*>(base);
+  p.error = reinterpret_cast<unsigned*>(base) + 1;
+  p.partials = reinterpret_cast<double*>(base + kWsHeader);
+
+  const int64_t max_grid = static_cast<int64_t>(st->sms) * st->occupancy[idx];
+  int64_t grid = 1;
+  if (v->kind == kKindBulk) {
+    // 16-byte bulk copies: an odd final row of an odd-width operand is left
+    // to the reduction epilogue.
+    p.rows_main = ((m % 2 == 0) && (k % 2 == 0)) ? n : (n & ~int64_t(1));
+    p.num_chunks = (p.rows_main + v->rows - 1) / v->rows;
+    grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, max_grid));
+  } else {
+    p.rows_main = n;
+    p.num_chunks = 0;
+    const int tiles = (v->wa / v->ta) * (v->wb / v->tb);
+    const int64_t row_groups = v->threads / tiles;
+    grid = std::max<int64_t>(1, std::min<int64_t>((n + row_groups - 1) / row_groups, max_grid));
+  }
+
+  void* args[] = {&p};
+  cudaError_t e = cudaLaunchKernel(v->kernel, dim3(static_cast<unsigned>(grid)), dim3(v->threads), args, v->smem,
+                                   stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernel");
+  return TSM_SUCCESS;
+}
+
+// ----------------------------------------------------------------- fills
+__global__ void fill_uniform_kernel(double* x, int64_t count, uint64_t seed, uint64_t stream_id) {
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += step) {
+    uint64_t z = seed + ((stream_id << 40) + static_cast<uint64_t>(i) + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = static_cast<double>(z >> 11) * 0x1.0p-53;
+    x[i] = 2.0 * u - 1.0;
+  }
+}
+
+}  // namespace
+}  // namespace tsm
+
+using namespace tsm;
+
+extern "C" {
+
+int tsm_version(void) { return 100; }
+
+const char* tsm_status_string(tsm_status s) {
+  switch (s) {
+    case TSM_SUCCESS: return "success";
+    case TSM_ERROR_INVALID_VALUE: return "invalid value (shape, pointer or leading dimension)";
+    case TSM_ERROR_WORKSPACE: return "workspace missing, unaligned or too small";
+    case TSM_ERROR_CUDA: return "CUDA runtime error";
+    case TSM_ERROR_UNSUPPORTED: return "no compiled variant supports this request";
+    case TSM_ERROR_DEVICE_TIMEOUT: return "a kernel gave up a bounded wait";
+  }
+  return "unknown status";
+}
+
+const char* tsm_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
+
+size_t tsm_gemm_tn_workspace_size(int64_t n, int m, int k) {
+  (void)n;
+  if (m < 1 || k < 1 || m > 64 || k > 64) return 0;
+  int dev = 0;
+  DeviceState* st = nullptr;
+  if (current_device(&dev, &st) != TSM_SUCCESS) return 0;
+  return workspace_bytes_for(st->sms, m, k);
+}
+
+tsm_status tsm_gemm_tn_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                           const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate, void* workspace,
+                           size_t workspace_bytes) {
+  return launch_plain(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate, workspace,
+                      workspace_bytes, -1);
+}
+
+tsm_status tsm_gemm_tn_f64_variant(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                                   const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
+                                   void* workspace, size_t workspace_bytes, int variant) {
+  return launch_plain(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate, workspace,
+                      workspace_bytes, variant);
+}
+
+int tsm_gemm_tn_default_variant(int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
+  if (check_args(n, m, k, A, lda, B, ldb, A ? A : B, k) != TSM_SUCCESS) return -1;
+  return default_variant(n, m, k, A, lda, B, ldb);
+}
+
+int tsm_variant_count(void) { return static_cast<int>(variants().size()); }
+
+tsm_status tsm_variant_get_info(int index, tsm_variant_info* info) {
+  if (index < 0 || index >= tsm_variant_count() || info == nullptr) return TSM_ERROR_INVALID_VALUE;
+  const Variant* v = variants()[index];
+  std::memset(info, 0, sizeof(*info));
+  std::strncpy(info->name, v->name, sizeof(info->name) - 1);
+  info->kind = v->kind;
+  info->wa = v->wa;
+  info->wb = v->wb;
+  info->ta = v->ta;
+  info->tb = v->tb;
+  info->exact = v->exact;
+  info->threads = v->threads;
+  info->stages = v->stages;
+  info->rows = v->rows;
+  info->unroll = v->unroll;
+  info->smem_bytes = v->smem;
+  return TSM_SUCCESS;
+}
+
+tsm_status tsm_workspace_check(tsm_stream_t stream, void* workspace, unsigned* bits) {
+  if (workspace == nullptr) return TSM_ERROR_WORKSPACE;
+  unsigned host = 0;
+  unsigned* err = static_cast<unsigned*>(workspace) + 1;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(&host, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(unsigned), s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "tsm_workspace_check");
+  if (bits) *bits = host;
+  return host ? TSM_ERROR_DEVICE_TIMEOUT : TSM_SUCCESS;
+}
+
+tsm_status tsm_fill_uniform_f64(tsm_stream_t stream, double* x, int64_t count, uint64_t seed, uint64_t stream_id) {
+  if (count < 0 || (count > 0 && x == nullptr)) return TSM_ERROR_INVALID_VALUE;
+  if (count == 0) return TSM_SUCCESS;
+  int dev = 0;
+  DeviceState* st = nullptr;
+  tsm_status s = current_device(&dev, &st);
+  if (s != TSM_SUCCESS) return s;
+  const int64_t blocks = std::min<int64_t>((count + 255) / 256, static_cast<int64_t>(st->sms) * 16);
+  fill_uniform_kernel<<<static_cast<unsigned>(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(x, count, seed,
+                                                                                                    stream_id);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fill_uniform_kernel");
+  return TSM_SUCCESS;
+}
+
+}  // extern "C"

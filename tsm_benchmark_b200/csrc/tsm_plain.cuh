@@ -1,0 +1,351 @@
+// tsm_plain.cuh -- the plain FP64 TSMTTSM kernels, C (m x k) = A^T * B with
+// A (n x m) and B (n x k) row-major.
+//
+// Replaces the nine SYCL kernels of tsmttsm.hh (and the generated ones of
+// sycl_codegen*.py).  All of them compute C[i][j] += sum_r A[r][i] * B[r][j]
+// with a per-work-item register tile and FP64 atomics into C; here:
+//
+//   * tsm_tn_bulk_kernel  -- persistent CTAs (one or two per SM).  A producer
+//     warp streams contiguous row chunks of A and B into a STAGES-deep ring of
+//     shared-memory buffers with 1-D TMA bulk copies (cp.async.bulk, mbarrier
+//     completion, L2 evict-first); CW consumer warps each own a TA x TB FP64
+//     register tile of C and walk the chunk's rows.  Needs lda == m,
+//     ldb == k and 16-byte aligned A and B.
+//   * tsm_tn_direct_kernel -- the same register tiles fed by plain read-only
+//     global loads; any lda/ldb and any alignment.
+//
+// Both end in the same deterministic two-level reduction in place of the
+// reference's atomics: warp shuffles and a fixed-order shared-memory sum give
+// one m x k partial per CTA, written to the workspace; the last CTA to finish
+// (a counter in the workspace) sums the partials in CTA order and writes C.
+// The result is therefore bit-identical from run to run for a given variant
+// and grid.  No value of C is ever updated atomically.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "tsm_device.cuh"
+
+namespace tsm {
+
+struct PlainArgs {
+  const double* A;
+  const double* B;
+  double* C;
+  int64_t n;  // rows of A and B
+  int m;      // columns of A = rows of C
+  int k;      // columns of B = columns of C
+  int64_t lda, ldb, ldc;
+  int accumulate;      // 1: C += A^T B (the reference's semantics), 0: C = A^T B
+  int64_t rows_main;   // rows covered by the main loop; rows [rows_main, n) are added at the end
+  int64_t num_chunks;  // bulk kernel: ceil(rows_main / RS)
+  double* partials;    // workspace: gridDim.x * m * k doubles
+  unsigned* counter;   // workspace: CTAs finished in this launch (zero between launches)
+  unsigned* error;     // workspace: sticky error bits (dev::kErr*)
+};
+
+// Compile-time shape of one register-tiled variant.
+//   WA, WB : widths (exact) or width capacities (EXACT == false; the actual
+//            m <= WA, k <= WB come at run time and columns beyond are masked)
+//   TA, TB : the per-thread tile of C, TA x TB
+template <int WA, int WB, int TA, int TB>
+struct TileShape {
+  static_assert(WA % TA == 0 && WB % TB == 0, "tile must divide the width");
+  static constexpr int QA = WA / TA;
+  static constexpr int QB = WB / TB;
+  static constexpr int NT = QA * QB;  // threads that together cover C once
+  static_assert((NT & (NT - 1)) == 0, "tile count must be a power of two");
+};
+
+namespace detail {
+
+// Sums the per-thread tiles of one CTA into `red`, then into this CTA's slot
+// of the workspace; the last CTA then writes C.  `red` must hold
+// slots * m * k doubles.  Called by all threads of the CTA (nthreads), of
+// which the first `cthreads` carry tiles.
+template <int TA, int TB, int NT, bool EXACT, int WA, int WB>
+__device__ __forceinline__ void finish_tiles(const PlainArgs& p, double (&acc)[TA][TB], int t, int cthreads,
+                                             int nthreads, double* red, unsigned* s_is_last) {
+  const int m = EXACT ? WA : p.m;
+  const int k = EXACT ? WB : p.k;
+  const int mk = m * k;
+  const int lane = t & 31;
+  const int tile = t % NT;
+  const int ta = tile % (WA / TA), tb = tile / (WA / TA);
+  const bool carrier = t < cthreads;
+
+  // 1. Warp level: lanes that share a tile differ by multiples of NT.
+  if (carrier && NT < 32) {
+#pragma unroll
+    for (int off = NT; off < 32; off <<= 1)
+#pragma unroll
+      for (int i = 0; i < TA; ++i)
+#pragma unroll
+        for (int j = 0; j < TB; ++j) acc[i][j] += __shfl_xor_sync(0xffffffffu, acc[i][j], off);
+  }
+  // 2. One slot per warp (NT < 32) or per row group (NT >= 32).
+  const int slots = NT < 32 ? cthreads / 32 : cthreads / NT;
+  if (carrier && (NT >= 32 || lane < NT)) {
+    const int slot = NT < 32 ? t / 32 : t / NT;
+    double* dst = red + slot * mk;
+#pragma unroll
+    for (int i = 0; i < TA; ++i) {
+      const int row = ta * TA + i;
+#pragma unroll
+      for (int j = 0; j < TB; ++j) {
+        const int col = tb * TB + j;
+        if (EXACT || (row < m && col < k)) dst[row * k + col] = acc[i][j];
+      }
+    }
+  }
+  __syncthreads();
+  // 3. Fixed-order sum over the slots -> this CTA's partial in the workspace.
+  double* mine = p.partials + static_cast<int64_t>(blockIdx.x) * mk;
+  for (int e = t; e < mk; e += nthreads) {
+    double s = red[e];
+    for (int q = 1; q < slots; ++q) s += red[q * mk + e];
+    mine[e] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (t == 0) {
+    const unsigned prev = atomicAdd(p.counter, 1u);
+    *s_is_last = (prev == gridDim.x - 1) ? 1u : 0u;
+  }
+  __syncthreads();
+  if (*s_is_last == 0u) return;
+
+  // 4. Last CTA: partials in CTA order, then the leftover rows, then C.
+  __threadfence();
+  const int G = gridDim.x;
+  for (int e = t; e < mk; e += nthreads) {
+    const int i = e / k, j = e - (e / k) * k;
+    double s = dev::ld_cg(p.partials + e);
+    for (int b = 1; b < G; ++b) s += dev::ld_cg(p.partials + static_cast<int64_t>(b) * mk + e);
+    for (int64_t r = p.rows_main; r < p.n; ++r) s += p.A[r * p.lda + i] * p.B[r * p.ldb + j];
+    double* c = p.C + static_cast<int64_t>(i) * p.ldc + j;
+    *c = p.accumulate ? *c + s : s;
+  }
+  if (t == 0) *p.counter = 0u;  // ready for the next launch on this workspace
+}
+
+// acc += a (TA) x b (TB) outer product.
+template <int TA, int TB>
+__device__ __forceinline__ void outer_fma(double (&acc)[TA][TB], const double (&a)[TA], const double (&b)[TB]) {
+#pragma unroll
+  for (int i = 0; i < TA; ++i)
+#pragma unroll
+    for (int j = 0; j < TB; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+}
+
+// Loads W consecutive doubles from shared memory (16-byte vector loads where
+// the layout allows) or, in capacity mode, up to `valid` of them (rest = 0).
+template <int W, bool VEC>
+__device__ __forceinline__ void load_row_seg(double (&v)[W], const double* src, int valid) {
+  if constexpr (VEC) {
+#pragma unroll
+    for (int i = 0; i < W / 2; ++i) {
+      const double2 x = reinterpret_cast<const double2*>(src)[i];
+      v[2 * i] = x.x;
+      v[2 * i + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) v[i] = (i < valid) ? src[i] : 0.0;
+  }
+}
+
+}  // namespace detail
+
+// --------------------------------------------------------------------------
+// Bulk (TMA) pipelined kernel.
+// --------------------------------------------------------------------------
+template <int WA, int WB, int TA, int TB, int CW, int STAGES, int RS, int UNROLL, bool EXACT>
+struct BulkKernel {
+  using S = TileShape<WA, WB, TA, TB>;
+  static constexpr int CT = CW * 32;         // consumer threads
+  static constexpr int THREADS = CT + 32;    // + one producer warp
+  static_assert(CT % S::NT == 0, "consumer threads must cover whole tiles");
+  static constexpr int RG = CT / S::NT;      // row groups
+  static_assert(RS % 2 == 0, "chunk rows must be even (16-byte bulk copies)");
+  static constexpr int STAGE_A = RS * WA;    // doubles (capacity)
+  static constexpr int STAGE_B = RS * WB;
+  static constexpr int SLOTS = S::NT < 32 ? CW : RG;
+  static constexpr size_t RING_BYTES = size_t(STAGES) * (STAGE_A + STAGE_B) * sizeof(double);
+  static constexpr size_t RED_BYTES = size_t(SLOTS) * WA * WB * sizeof(double);
+  static constexpr size_t DATA_BYTES = RING_BYTES > RED_BYTES ? RING_BYTES : RED_BYTES;
+  static constexpr size_t BAR_OFFSET = (DATA_BYTES + 127) / 128 * 128;
+  static constexpr size_t SMEM_BYTES = BAR_OFFSET + 2 * STAGES * sizeof(uint64_t) + 16;
+  static constexpr bool VEC_A = EXACT && TA % 2 == 0 && WA % 2 == 0;
+  static constexpr bool VEC_B = EXACT && TB % 2 == 0 && WB % 2 == 0;
+};
+
+template <int WA, int WB, int TA, int TB, int CW, int STAGES, int RS, int UNROLL, bool EXACT>
+__global__ void __launch_bounds__(BulkKernel<WA, WB, TA, TB, CW, STAGES, RS, UNROLL, EXACT>::THREADS, 1)
+    tsm_tn_bulk_kernel(const PlainArgs p) {
+  using K = BulkKernel<WA, WB, TA, TB, CW, STAGES, RS, UNROLL, EXACT>;
+  using S = typename K::S;
+  extern __shared__ __align__(128) unsigned char smem[];
+  double* ringA = reinterpret_cast<double*>(smem);
+  double* ringB = ringA + STAGES * K::STAGE_A;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + K::BAR_OFFSET);
+  uint64_t* empty = full + STAGES;
+  volatile int* abort = reinterpret_cast<volatile int*>(empty + STAGES);
+  unsigned* s_is_last = reinterpret_cast<unsigned*>(empty + STAGES) + 1;
+
+  const int t = threadIdx.x;
+  const int warp = t >> 5, lane = t & 31;
+  const int m = EXACT ? WA : p.m;
+  const int k = EXACT ? WB : p.k;
+
+  if (t == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      dev::mbar_init(&full[s], 1);
+      dev::mbar_init(&empty[s], CW);
+    }
+    *abort = 0;
+    dev::fence_mbar_init();
+  }
+  __syncthreads();
+
+  const int64_t G = gridDim.x;
+  double acc[TA][TB];
+#pragma unroll
+  for (int i = 0; i < TA; ++i)
+#pragma unroll
+    for (int j = 0; j < TB; ++j) acc[i][j] = 0.0;
+
+  if (warp == CW) {
+    // ---------------- producer warp: lane 0 issues, the warp stays converged.
+    int64_t issued = 0;
+    const uint64_t policy = dev::policy_evict_first();
+    for (int64_t c = blockIdx.x; c < p.num_chunks; c += G, ++issued) {
+      const int s = static_cast<int>(issued % STAGES);
+      const int64_t round = issued / STAGES;
+      bool ok = true;
+      if (lane == 0) {
+        if (round > 0) ok = dev::mbar_wait(&empty[s], static_cast<uint32_t>((round - 1) & 1), abort);
+        if (ok) {
+          const int64_t r0 = c * RS;
+          const int64_t rows = (p.rows_main - r0) < RS ? (p.rows_main - r0) : RS;
+          const uint32_t ba = static_cast<uint32_t>(rows * m * sizeof(double));
+          const uint32_t bb = static_cast<uint32_t>(rows * k * sizeof(double));
+          dev::mbar_arrive_expect_tx(&full[s], ba + bb);
+          dev::bulk_g2s_evict_first(ringA + s * K::STAGE_A, p.A + r0 * m, ba, &full[s], policy);
+          dev::bulk_g2s_evict_first(ringB + s * K::STAGE_B, p.B + r0 * k, bb, &full[s], policy);
+        } else {
+          *abort = 1;
+          atomicOr(p.error, dev::kErrTimeout);
+        }
+      }
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) break;
+    }
+  } else {
+    // ---------------- consumer warps.
+    const int tile = t % S::NT;
+    const int ta = tile % S::QA, tb = tile / S::QA;
+    const int rg = t / S::NT;
+    const int colA = ta * TA, colB = tb * TB;
+    const int validA = m - colA, validB = k - colB;
+    int64_t it = 0;
+    for (int64_t c = blockIdx.x; c < p.num_chunks; c += G, ++it) {
+      const int s = static_cast<int>(it % STAGES);
+      if (!dev::mbar_wait(&full[s], static_cast<uint32_t>((it / STAGES) & 1), abort)) {
+        *abort = 1;
+        atomicOr(p.error, dev::kErrTimeout);
+        break;
+      }
+      const int64_t r0 = c * RS;
+      const int rows = static_cast<int>((p.rows_main - r0) < RS ? (p.rows_main - r0) : RS);
+      const double* sa = ringA + s * K::STAGE_A + colA;
+      const double* sb = ringB + s * K::STAGE_B + colB;
+      if (rows == RS) {
+        static_assert((RS / K::RG) % UNROLL == 0 || RS < K::RG, "unroll must divide the rows per thread");
+#pragma unroll UNROLL
+        for (int r = rg; r < RS; r += K::RG) {
+          double a[TA], b[TB];
+          detail::load_row_seg<TA, K::VEC_A>(a, sa + r * m, validA);
+          detail::load_row_seg<TB, K::VEC_B>(b, sb + r * k, validB);
+          detail::outer_fma<TA, TB>(acc, a, b);
+        }
+      } else {
+        for (int r = rg; r < rows; r += K::RG) {
+          double a[TA], b[TB];
+          detail::load_row_seg<TA, K::VEC_A>(a, sa + r * m, validA);
+          detail::load_row_seg<TB, K::VEC_B>(b, sb + r * k, validB);
+          detail::outer_fma<TA, TB>(acc, a, b);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) dev::mbar_arrive(&empty[s]);
+    }
+  }
+
+  __syncthreads();
+  if (*abort && warp == CW && lane == 0) {
+    // Let every bulk copy this CTA issued land before the ring is reused or
+    // the CTA exits.  Bounded as well; a second timeout is only recorded.
+    int64_t issued = 0;
+    for (int64_t c = blockIdx.x; c < p.num_chunks; c += G) ++issued;
+    volatile int no_abort = 0;
+    for (int64_t q = issued > STAGES ? issued - STAGES : 0; q < issued; ++q)
+      if (!dev::mbar_wait(&full[q % STAGES], static_cast<uint32_t>((q / STAGES) & 1), &no_abort)) break;
+  }
+  __syncthreads();
+
+  detail::finish_tiles<TA, TB, S::NT, EXACT, WA, WB>(p, acc, t, K::CT, K::THREADS,
+                                                       reinterpret_cast<double*>(smem), s_is_last);
+}
+
+// --------------------------------------------------------------------------
+// Direct-load kernel (strided or unaligned operands).
+// --------------------------------------------------------------------------
+template <int WA, int WB, int TA, int TB, int THREADS, bool EXACT>
+struct DirectKernel {
+  using S = TileShape<WA, WB, TA, TB>;
+  static_assert(THREADS % S::NT == 0 && THREADS % 32 == 0, "threads must cover whole tiles");
+  static constexpr int RG = THREADS / S::NT;
+  static constexpr int SLOTS = S::NT < 32 ? THREADS / 32 : RG;
+  static constexpr size_t SMEM_BYTES = size_t(SLOTS) * WA * WB * sizeof(double) + 16;
+};
+
+template <int WA, int WB, int TA, int TB, int THREADS, bool EXACT>
+__global__ void __launch_bounds__(THREADS) tsm_tn_direct_kernel(const PlainArgs p) {
+  using K = DirectKernel<WA, WB, TA, TB, THREADS, EXACT>;
+  using S = typename K::S;
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned* s_is_last = reinterpret_cast<unsigned*>(smem + K::SMEM_BYTES - 16);
+
+  const int t = threadIdx.x;
+  const int m = EXACT ? WA : p.m;
+  const int k = EXACT ? WB : p.k;
+  const int tile = t % S::NT;
+  const int ta = tile % S::QA, tb = tile / S::QA;
+  const int colA = ta * TA, colB = tb * TB;
+  const int validA = m - colA, validB = k - colB;
+
+  double acc[TA][TB];
+#pragma unroll
+  for (int i = 0; i < TA; ++i)
+#pragma unroll
+    for (int j = 0; j < TB; ++j) acc[i][j] = 0.0;
+
+  const int64_t rstep = static_cast<int64_t>(gridDim.x) * K::RG;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * K::RG + t / S::NT; r < p.rows_main; r += rstep) {
+    const double* ar = p.A + r * p.lda + colA;
+    const double* br = p.B + r * p.ldb + colB;
+    double a[TA], b[TB];
+#pragma unroll
+    for (int i = 0; i < TA; ++i) a[i] = (EXACT || i < validA) ? __ldg(ar + i) : 0.0;
+#pragma unroll
+    for (int j = 0; j < TB; ++j) b[j] = (EXACT || j < validB) ? __ldg(br + j) : 0.0;
+    detail::outer_fma<TA, TB>(acc, a, b);
+  }
+  detail::finish_tiles<TA, TB, S::NT, EXACT, WA, WB>(p, acc, t, THREADS, THREADS,
+                                                       reinterpret_cast<double*>(smem), s_is_last);
+}
+
+}  // namespace tsm

@@ -1,0 +1,56 @@
+// tsm_registry.cuh -- the table of compiled kernel variants.
+//
+// The reference picks its launch shape through template parameters and
+// generated kernel names (tsmttsm.hh: <M, stride, local_size, tile>;
+// sycl_codegen_new.py:153 names tsmttsm_{M}_{N}_{TM}_{TN}{,_lf,_sg,_sg_lf}).
+// Here every compiled configuration is one row of a table, written by
+// tsm_benchmark_b200/codegen.py into csrc/generated/; the host dispatcher and
+// the autotuner choose rows by index.
+#pragma once
+
+#include <cstddef>
+
+#include "tsm_plain.cuh"
+
+namespace tsm {
+
+enum VariantKind : int { kKindBulk = 0, kKindDirect = 1 };
+
+struct Variant {
+  const char* name;
+  int kind;     // VariantKind
+  int wa, wb;   // widths (exact) or capacities
+  int ta, tb;   // per-thread tile of C
+  int exact;    // 1: only m == wa && k == wb; 0: any m <= wa, k <= wb
+  int threads;  // CTA size
+  int stages;   // bulk: shared-memory ring depth
+  int rows;     // bulk: rows per chunk (RS)
+  int unroll;   // bulk: row-loop unroll
+  size_t smem;  // dynamic shared memory per CTA
+  const void* kernel;
+};
+
+struct VariantPart {
+  const Variant* rows;
+  int count;
+};
+
+// Parts written by the generator (csrc/generated/variants_index.cu).
+extern const VariantPart kVariantParts[];
+extern const int kVariantPartCount;
+
+}  // namespace tsm
+
+#define TSM_BULK_VARIANT(NAME, WA, WB, TA, TB, CW, ST, RS, U, EX)                                       \
+  ::tsm::Variant {                                                                                    \
+    NAME, ::tsm::kKindBulk, WA, WB, TA, TB, EX, ::tsm::BulkKernel<WA, WB, TA, TB, CW, ST, RS, U, EX>::THREADS, \
+        ST, RS, U, ::tsm::BulkKernel<WA, WB, TA, TB, CW, ST, RS, U, EX>::SMEM_BYTES,                   \
+        reinterpret_cast<const void*>(&::tsm::tsm_tn_bulk_kernel<WA, WB, TA, TB, CW, ST, RS, U, EX>)  \
+  }
+
+#define TSM_DIRECT_VARIANT(NAME, WA, WB, TA, TB, TH, EX)                                              \
+  ::tsm::Variant {                                                                                    \
+    NAME, ::tsm::kKindDirect, WA, WB, TA, TB, EX, TH, 0, 0, 1,                                        \
+        ::tsm::DirectKernel<WA, WB, TA, TB, TH, EX>::SMEM_BYTES,                                      \
+        reinterpret_cast<const void*>(&::tsm::tsm_tn_direct_kernel<WA, WB, TA, TB, TH, EX>)           \
+  }
