@@ -50,6 +50,14 @@ def test_generated_sources_current():
     from tsm_benchmark_b200 import codegen
     files = codegen.render(codegen.default_variants(), codegen.load_tuned())
     assert codegen.is_current(files), "run python -m tsm_benchmark_b200.codegen"
+    compat = codegen.render_compat_header(codegen.default_variants())
+    assert open(codegen.COMPAT_HEADER).read() == compat
+    # the names the reference's v2 generator emits by default (sycl_codegen_new.py:645-661)
+    for m in (4, 8, 16):
+        for tm in (2, 4):
+            for suffix in ("", "_lf", "_sg", "_sg_lf"):
+                assert f"sycl::event tsmttsm_{m}_{m}_{tm}_{tm}{suffix}(" in compat
+    assert "void run_all_benchmarks(sycl::queue& q, int K = 1 << 20, int warmup = 10, int runs = 30)" in compat
 
 
 def test_generator_rejects_bad_variants():

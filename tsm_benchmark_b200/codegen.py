@@ -280,6 +280,74 @@ def render(vs: list, tuned: list, parts: int = 8) -> dict[str, str]:
     return files
 
 
+COMPAT_HEADER = os.path.join(HERE, "compat", "tsmttsm_kernels.hh")
+COMPAT_SUFFIXES = ("", "_lf", "_sg", "_sg_lf")
+
+
+def compat_variant_for(vs: list, m: int, tm: int) -> str | None:
+    """The exact bulk variant whose register tile is the reference's TM x TM
+    for width m, else None (the library default is used)."""
+    for v in vs:
+        if isinstance(v, BulkVariant) and v.exact and (v.wa, v.wb, v.ta, v.tb) == (m, m, tm, tm) \
+                and v.unroll == 1 and v.cw == 8 and v.stages == 6:
+            return v.name
+    return None
+
+
+def render_compat_header(vs: list, widths=(4, 8, 16), tiles=(2, 4)) -> str:
+    """tsmttsm_kernels.hh for main_codegen.cc: the names sycl_codegen_new.py
+    emits (tsmttsm_{M}_{N}_{TM}_{TN}{,_lf,_sg,_sg_lf}, :153,:257) with its
+    signature (q, int K, const T* A, const T* B, T* C) (:159,:264), each a
+    library call pinned to the variant with the same register tile, and
+    run_all_benchmarks<T>(q, K, warmup, runs) (:417-419)."""
+    out = [HEADER.rstrip("\n"), "//",
+           "// Drop-in for the header `sycl_codegen_new.py --with-benchmark` emits.",
+           "// Kernel names and signatures are the reference generator's; every kernel",
+           "// adds A^T B into C through tsm_gemm_tn_f64_variant on the queue's stream.",
+           "// The _lf / _sg / _sg_lf spellings name the reference's prefetch and",
+           "// sub-group-reduction options; every variant here prefetches through a",
+           "// multi-stage TMA ring and reduces with warp shuffles, so they share one",
+           "// variant per (M, TM).",
+           "#pragma once", "", "#include <sycl/sycl.hpp>", "", "#include <vector>", "",
+           '#include "tsm_compat_bench.hh"', '#include "tsmttsm.hh"', ""]
+    for m in widths:
+        for tm in tiles:
+            if m % tm:
+                continue
+            vname = compat_variant_for(vs, m, tm)
+            for suffix in COMPAT_SUFFIXES:
+                fname = f"tsmttsm_{m}_{m}_{tm}_{tm}{suffix}"
+                out.append("template <typename T>")
+                out.append(f"sycl::event {fname}(sycl::queue& q, int K, const T* A, const T* B, T* C) {{")
+                if vname:
+                    out.append(f'  static const int variant = tsm_compat::variant_by_name("{vname}");')
+                else:
+                    out.append("  static const int variant = -1;  // no variant with this tile: library default")
+                out.append(f"  return tsm_compat::accumulate_tn<T>(q, K, {m}, {m}, A, B, C, variant);")
+                out.append("}")
+                out.append("")
+    out.append("template <typename T>")
+    out.append("void run_all_benchmarks(sycl::queue& q, int K = 1 << 20, int warmup = 10, int runs = 30) {")
+    out.append('  std::cout << "Device: " << q.get_device().get_info<sycl::info::device::name>() << "\\n\\n";')
+    out.append("  std::vector<tsm_compat::BenchResult> results;")
+    for m in widths:
+        out.append("  {")
+        out.append(f"    tsm_compat::Problem<T> p(q, K, {m});")
+        for tm in tiles:
+            if m % tm:
+                continue
+            for suffix, label in zip(COMPAT_SUFFIXES, ("basic", "lf", "sg", "sg_lf")):
+                fname = f"tsmttsm_{m}_{m}_{tm}_{tm}{suffix}"
+                out.append(f'    results.push_back(p.bench("M{m}_T{tm}_{label}", '
+                           f"[&](int k) {{ return {fname}<T>(q, k, p.A, p.B, p.C); }}, warmup, runs));")
+        out.append("  }")
+    out.append("  tsm_compat::print_results(results);")
+    out.append("}")
+    out.append("")
+    out.append("// End of generated code")
+    return "\n".join(out) + "\n"
+
+
 def write(files: dict[str, str], out_dir: str = GEN_DIR) -> None:
     os.makedirs(out_dir, exist_ok=True)
     for name, text in files.items():
@@ -309,15 +377,19 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     vs = default_variants()
     files = render(vs, load_tuned())
+    compat = render_compat_header(vs)
     if args.list:
         for v in vs:
             print(v.name)
         return 0
     if args.check:
-        ok = is_current(files, args.out)
+        ok = is_current(files, args.out) and os.path.exists(COMPAT_HEADER) and open(COMPAT_HEADER).read() == compat
         print("generated kernels are", "current" if ok else "STALE")
         return 0 if ok else 1
     write(files, args.out)
+    if not os.path.exists(COMPAT_HEADER) or open(COMPAT_HEADER).read() != compat:
+        with open(COMPAT_HEADER, "w") as f:
+            f.write(compat)
     print(f"wrote {len(files)} files, {len(vs)} variants, {len(load_tuned())} tuned choices to {args.out}")
     return 0
 

@@ -1,0 +1,204 @@
+// Generated by tsm_benchmark_b200/codegen.py -- do not edit.
+// Regenerate with: python -m tsm_benchmark_b200.codegen
+//
+// Drop-in for the header `sycl_codegen_new.py --with-benchmark` emits.
+// Kernel names and signatures are the reference generator's; every kernel
+// adds A^T B into C through tsm_gemm_tn_f64_variant on the queue's stream.
+// The _lf / _sg / _sg_lf spellings name the reference's prefetch and
+// sub-group-reduction options; every variant here prefetches through a
+// multi-stage TMA ring and reduces with warp shuffles, so they share one
+// variant per (M, TM).
+#pragma once
+
+#include <sycl/sycl.hpp>
+
+#include <vector>
+
+#include "tsm_compat_bench.hh"
+#include "tsmttsm.hh"
+
+template <typename T>
+sycl::event tsmttsm_4_4_2_2(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_4x4_t2x2_w8_s6_r512_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 4, 4, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_4_4_2_2_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_4x4_t2x2_w8_s6_r512_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 4, 4, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_4_4_2_2_sg(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_4x4_t2x2_w8_s6_r512_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 4, 4, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_4_4_2_2_sg_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_4x4_t2x2_w8_s6_r512_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 4, 4, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_4_4_4_4(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_4x4_t4x4_w8_s6_r512_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 4, 4, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_4_4_4_4_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_4x4_t4x4_w8_s6_r512_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 4, 4, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_4_4_4_4_sg(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_4x4_t4x4_w8_s6_r512_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 4, 4, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_4_4_4_4_sg_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_4x4_t4x4_w8_s6_r512_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 4, 4, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_8_8_2_2(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = -1;  // no variant with this tile: library default
+  return tsm_compat::accumulate_tn<T>(q, K, 8, 8, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_8_8_2_2_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = -1;  // no variant with this tile: library default
+  return tsm_compat::accumulate_tn<T>(q, K, 8, 8, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_8_8_2_2_sg(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = -1;  // no variant with this tile: library default
+  return tsm_compat::accumulate_tn<T>(q, K, 8, 8, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_8_8_2_2_sg_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = -1;  // no variant with this tile: library default
+  return tsm_compat::accumulate_tn<T>(q, K, 8, 8, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_8_8_4_4(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_8x8_t4x4_w8_s6_r256_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 8, 8, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_8_8_4_4_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_8x8_t4x4_w8_s6_r256_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 8, 8, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_8_8_4_4_sg(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_8x8_t4x4_w8_s6_r256_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 8, 8, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_8_8_4_4_sg_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_8x8_t4x4_w8_s6_r256_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 8, 8, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_16_16_2_2(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = -1;  // no variant with this tile: library default
+  return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_16_16_2_2_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = -1;  // no variant with this tile: library default
+  return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_16_16_2_2_sg(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = -1;  // no variant with this tile: library default
+  return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_16_16_2_2_sg_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = -1;  // no variant with this tile: library default
+  return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_16_16_4_4(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_16x16_t4x4_w8_s6_r128_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_16_16_4_4_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_16x16_t4x4_w8_s6_r128_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_16_16_4_4_sg(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_16x16_t4x4_w8_s6_r128_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant);
+}
+
+template <typename T>
+sycl::event tsmttsm_16_16_4_4_sg_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
+  static const int variant = tsm_compat::variant_by_name("bulk_16x16_t4x4_w8_s6_r128_u1");
+  return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant);
+}
+
+template <typename T>
+void run_all_benchmarks(sycl::queue& q, int K = 1 << 20, int warmup = 10, int runs = 30) {
+  std::cout << "Device: " << q.get_device().get_info<sycl::info::device::name>() << "\n\n";
+  std::vector<tsm_compat::BenchResult> results;
+  {
+    tsm_compat::Problem<T> p(q, K, 4);
+    results.push_back(p.bench("M4_T2_basic", [&](int k) { return tsmttsm_4_4_2_2<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M4_T2_lf", [&](int k) { return tsmttsm_4_4_2_2_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M4_T2_sg", [&](int k) { return tsmttsm_4_4_2_2_sg<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M4_T2_sg_lf", [&](int k) { return tsmttsm_4_4_2_2_sg_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M4_T4_basic", [&](int k) { return tsmttsm_4_4_4_4<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M4_T4_lf", [&](int k) { return tsmttsm_4_4_4_4_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M4_T4_sg", [&](int k) { return tsmttsm_4_4_4_4_sg<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M4_T4_sg_lf", [&](int k) { return tsmttsm_4_4_4_4_sg_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+  }
+  {
+    tsm_compat::Problem<T> p(q, K, 8);
+    results.push_back(p.bench("M8_T2_basic", [&](int k) { return tsmttsm_8_8_2_2<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M8_T2_lf", [&](int k) { return tsmttsm_8_8_2_2_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M8_T2_sg", [&](int k) { return tsmttsm_8_8_2_2_sg<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M8_T2_sg_lf", [&](int k) { return tsmttsm_8_8_2_2_sg_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M8_T4_basic", [&](int k) { return tsmttsm_8_8_4_4<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M8_T4_lf", [&](int k) { return tsmttsm_8_8_4_4_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M8_T4_sg", [&](int k) { return tsmttsm_8_8_4_4_sg<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M8_T4_sg_lf", [&](int k) { return tsmttsm_8_8_4_4_sg_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+  }
+  {
+    tsm_compat::Problem<T> p(q, K, 16);
+    results.push_back(p.bench("M16_T2_basic", [&](int k) { return tsmttsm_16_16_2_2<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M16_T2_lf", [&](int k) { return tsmttsm_16_16_2_2_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M16_T2_sg", [&](int k) { return tsmttsm_16_16_2_2_sg<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M16_T2_sg_lf", [&](int k) { return tsmttsm_16_16_2_2_sg_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M16_T4_basic", [&](int k) { return tsmttsm_16_16_4_4<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M16_T4_lf", [&](int k) { return tsmttsm_16_16_4_4_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M16_T4_sg", [&](int k) { return tsmttsm_16_16_4_4_sg<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+    results.push_back(p.bench("M16_T4_sg_lf", [&](int k) { return tsmttsm_16_16_4_4_sg_lf<T>(q, k, p.A, p.B, p.C); }, warmup, runs));
+  }
+  tsm_compat::print_results(results);
+}
+
+// End of generated code
