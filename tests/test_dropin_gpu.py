@@ -40,5 +40,5 @@ def test_main_codegen_dropin(gpu):
     PASSes the generated harness's check (all K rows)."""
     out = run("main_codegen_dropin")
     rows = re.findall(r"^\s*(M\d+_T\d+_\w+)\s+(PASS|FAIL)", out, flags=re.M)
-    assert len(rows) == 20, out[-3000:]
+    assert len(rows) == 24, out[-3000:]  # 3 widths x 2 tiles x 4 names
     assert all(s == "PASS" for _, s in rows), out[-3000:]

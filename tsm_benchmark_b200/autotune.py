@@ -1,0 +1,127 @@
+#!/usr/bin/env python3
+"""Autotuner: picks the fastest compiled variant per (m, k, n-bucket, dtype).
+
+    python -m tsm_benchmark_b200.autotune [--shapes sweep|batched|all] [--out tuned.json]
+
+For every width pair and row bucket it times each applicable variant of the
+table (CUDA events, warm-up then repeated launches, inputs larger than L2
+where the bucket allows), checks every candidate against the first one's
+result (the checksum identity and a normwise bound), and records the winner.
+The result, ``tsm_benchmark_b200/tuned.json``, is baked into the library's
+default choice by the next build (codegen.py reads it); until then the API's
+``variant=`` argument can use it directly.
+
+Replaces the reference's manual search over launch shapes (main.cc:171-192:
+M x stride x tile) and its generator's stride helpers (suggest_stride /
+validate_stride, sycl_codegen_new.py:530-580).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_OUT = os.path.join(HERE, "tuned.json")
+
+SWEEP_PAIRS = [(1, 1), (2, 2), (4, 4), (8, 8), (16, 16), (32, 32), (64, 64), (4, 32), (32, 4), (1, 64)]
+BATCHED_PAIRS = [(a, b) for a in (4, 8, 16, 32) for b in (4, 8, 16, 32)]
+# (nmin, n to time at): the largest nmin <= n selects the entry at run time.
+BUCKETS = [(0, 1 << 15), (1 << 18, 1 << 20), (1 << 23, 1 << 26)]
+MAX_BYTES = 24 << 30  # per operand pair while tuning
+
+
+def candidates(variants: list[dict], m: int, k: int) -> list[dict]:
+    out = []
+    for v in variants:
+        fits = (m == v["wa"] and k == v["wb"]) if v["exact"] else (m <= v["wa"] and k <= v["wb"])
+        if fits:
+            out.append(v)
+    return out
+
+
+def time_variant(call, reps: int, warmup: int = 3) -> float:
+    import torch
+    for _ in range(warmup):
+        call()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tune(pairs, buckets=BUCKETS, reps_time_ms: float = 150.0, verbose: bool = True) -> dict:
+    import torch
+
+    from . import variants as list_variants
+    from .api import fill_uniform, tsmttsm
+
+    dev = torch.device("cuda", 0)
+    vs = list_variants()
+    choices, timings = [], {}
+    for m, k in pairs:
+        for nmin, n in buckets:
+            while n > 1 << 12 and 8 * n * (m + k) > MAX_BYTES:
+                n //= 2
+            A = torch.empty((n, m), dtype=torch.float64, device=dev)
+            B = torch.empty((n, k), dtype=torch.float64, device=dev)
+            fill_uniform(A, 3, 0)
+            fill_uniform(B, 3, 1)
+            chk = float((A.sum(1) * B.sum(1)).sum())
+            bound = 8 * math.sqrt(n) * 2.0**-53 * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B))
+            C = torch.empty((m, k), dtype=torch.float64, device=dev)
+            ref = None
+            best = None
+            row = {}
+            for v in candidates(vs, m, k):
+                call = lambda: tsmttsm(A, B, C, variant=v["index"])  # noqa: E731
+                t0 = time_variant(call, 1, warmup=1)
+                reps = max(3, min(200, int(reps_time_ms / max(t0, 1e-3))))
+                ms = time_variant(call, reps)
+                got = C.clone()
+                if ref is None:
+                    ref = got
+                ok = abs(float(got.sum()) - chk) <= bound * math.sqrt(m * k) and \
+                    float(torch.linalg.norm(got - ref)) <= 2 * bound
+                gbs = 8 * n * (m + k) / (ms * 1e-3) / 1e9
+                row[v["name"]] = {"ms": round(ms, 5), "GB/s": round(gbs, 1), "ok": ok}
+                if ok and (best is None or ms < best[1]):
+                    best = (v["name"], ms, gbs)
+            timings[f"{m}x{k}@{n}"] = row
+            if best:
+                choices.append({"m": m, "k": k, "nmin": nmin, "n_timed": n, "variant": best[0],
+                                "ms": round(best[1], 5), "GB/s": round(best[2], 1)})
+                if verbose:
+                    print(f"{m:>2}x{k:<2} n={n:>9}: {best[0]:<40} {best[2]:8.1f} GB/s "
+                          f"({len(row)} candidates)", flush=True)
+            del A, B
+            torch.cuda.empty_cache()
+    return {"device": torch.cuda.get_device_name(dev), "dtype": "f64", "when": time.strftime("%Y-%m-%d %H:%M:%S"),
+            "choices": choices, "timings": timings}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--shapes", choices=["sweep", "batched", "all"], default="all")
+    ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--budget-ms", type=float, default=150.0, help="timed milliseconds per candidate")
+    args = ap.parse_args(argv)
+    pairs = {"sweep": SWEEP_PAIRS, "batched": BATCHED_PAIRS,
+             "all": sorted(set(SWEEP_PAIRS + BATCHED_PAIRS))}[args.shapes]
+    res = tune(pairs, reps_time_ms=args.budget_ms)
+    with open(args.out, "w") as f:
+        json.dump(res, f, indent=1)
+        f.write("\n")
+    print(f"wrote {args.out}: {len(res['choices'])} choices")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

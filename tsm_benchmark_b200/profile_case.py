@@ -1,0 +1,57 @@
+#!/usr/bin/env python3
+"""Runs one TSMTTSM shape a few times -- a small, self-contained case to put
+under a profiler (ncu) or to time one variant.
+
+    python -m tsm_benchmark_b200.profile_case --n 4194304 --m 8 --k 8 --reps 4 [--variant NAME]
+
+Inputs are generated on the device (the library's uniform generator); the
+last result is checked against the checksum identity
+sum_ij C_ij = sum_r (sum_i A_ri)(sum_j B_rj).
+"""
+from __future__ import annotations
+
+import argparse
+import math
+import sys
+
+import torch
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=1 << 22)
+    ap.add_argument("--m", type=int, default=8)
+    ap.add_argument("--k", type=int, default=8)
+    ap.add_argument("--reps", type=int, default=4)
+    ap.add_argument("--variant", default=None, help="variant name (default: the library's choice)")
+    args = ap.parse_args(argv)
+
+    from tsm_benchmark_b200 import fill_uniform, tsmttsm, variants
+    dev = torch.device("cuda", 0)
+    A = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
+    B = torch.empty((args.n, args.k), dtype=torch.float64, device=dev)
+    fill_uniform(A, 1, 0)
+    fill_uniform(B, 1, 1)
+    vidx = -1
+    if args.variant:
+        names = {v["name"]: v["index"] for v in variants()}
+        vidx = names[args.variant]
+    C = None
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.reps):
+        C = tsmttsm(A, B, variant=vidx)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.reps
+    gbs = 8 * args.n * (args.m + args.k) / (ms * 1e-3) / 1e9
+    chk = float((A.sum(1) * B.sum(1)).sum())
+    bound = 32 * math.sqrt(args.n) * 2.0**-53 * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B))
+    ok = abs(float(C.sum()) - chk) <= bound * math.sqrt(args.m * args.k)
+    print(f"n={args.n} m={args.m} k={args.k} reps={args.reps}: {ms:.4f} ms/call, {gbs:.1f} GB/s, checksum "
+          f"{'ok' if ok else 'MISMATCH'}")
+    return 0 if ok else 1
+
+
+if __name__ == "__main__":
+    sys.exit(main())
