@@ -106,6 +106,26 @@ tsm_status tsm_variant_get_info(int index, tsm_variant_info* info);
  * not valid; the call then returns TSM_ERROR_DEVICE_TIMEOUT. */
 tsm_status tsm_workspace_check(tsm_stream_t stream, void* workspace, unsigned* bits);
 
+/* C = A^T B (accumulate = 0) or C += A^T B (accumulate = 1), FP64, WITHOUT a
+ * workspace.  No counterpart in the reference (its SYCL kernels need no
+ * scratch because they add into C with atomics).  For callers that cannot
+ * allocate device memory or own a workspace -- a plug-in whose host program
+ * owns every device allocation, or a latency-bound loop where cudaMalloc
+ * (which may synchronise the device) is not allowed -- this entry point
+ * allocates nothing: its scratch is a 4 MiB array inside the library that
+ * every GPU loading the library holds until exit.  Same variant choice and
+ * result as tsm_gemm_tn_f64.  Limit: the call needs 256 + CTAs * m * k * 8
+ * bytes of that array.  On a 148-SM B200 with contiguous, 16-byte aligned
+ * operands (one CTA per SM) that admits any n for m * k <= 3542, and 64 x 64
+ * up to about 4,000 rows; strided or unaligned operands (up to four CTAs per
+ * SM) admit any n for m * k <= 885.  Larger requests return
+ * TSM_ERROR_WORKSPACE and launch nothing.  All calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller.  The
+ * first call on each device looks up the array's device address; make it
+ * before any stream capture.  Device error bits are not reported. */
+tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                                   const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate);
+
 /* Benchmark-input generator: x[i] = 2u - 1 in [-1, 1), u the top 53 bits of
  * SplitMix64 at counter (stream_id * 2^40 + i + 1) under `seed`.  The same
  * values as the oracle's host generator, bit for bit, independent of the

@@ -67,6 +67,8 @@ SIGNATURES = {
     "tsm_variant_get_info": (c_int, [c_int, ctypes.POINTER(VariantInfo)]),
     "tsm_workspace_check": (c_int, [c_void_p, c_void_p, ctypes.POINTER(ctypes.c_uint)]),
     "tsm_fill_uniform_f64": (c_int, [c_void_p, c_void_p, c_int64, c_uint64, c_uint64]),
+    "tsm_gemm_tn_f64_noalloc": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                        c_void_p, c_int64, c_int]),
 }
 
 _lib = None

@@ -328,3 +328,121 @@ tsm_status tsm_fill_uniform_f64(tsm_stream_t stream, double* x, int64_t count, u
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point: tsm_gemm_tn_f64_noalloc.
+//
+// Some callers cannot hand the library a workspace.  A plugin loaded into a
+// host program that owns every device allocation (its own pool, no
+// cudaMalloc from plug-ins), or a latency-bound loop where a cudaMalloc --
+// which may synchronise the whole device -- is not allowed after start-up,
+// can still call this.  The scratch the kernels need (a launch counter, an
+// error word and one m x k partial per CTA) lives in the file-scope array
+// below instead, which every GPU that loads this library holds until the
+// process exits.
+//
+// Limits and sharing:
+//   * kStaticScratchBytes (4 MiB) bounds a call: 256 B of header plus
+//     (CTAs launched) * m * k * 8 B of partials.  A request that would need
+//     more returns TSM_ERROR_WORKSPACE and runs nothing.
+//   * All calls on a device share the one array and it keeps whatever the
+//     last call left.  The launch counter must start at zero, so each call
+//     zeroes it (stream-ordered) before its launch.  Calls that overlap on
+//     the GPU (different streams, other threads) race on the array and give
+//     wrong results: serialise them.
+//   * The first call on each device looks the array's device address up
+//     (cudaGetSymbolAddress, with that device current); make that first call
+//     before any stream capture.
+// ---------------------------------------------------------------------------
+namespace tsm {
+namespace {
+constexpr size_t kStaticScratchBytes = size_t(4) << 20;
+constexpr int kStaticScratchDevices = 64;
+}  // namespace
+}  // namespace tsm
+
+static __device__ __align__(256) unsigned char tsm_static_scratch[tsm::kStaticScratchBytes];
+
+namespace tsm {
+namespace {
+
+std::mutex g_static_mu;
+void* g_static_ptr[kStaticScratchDevices] = {};
+
+// Device address of tsm_static_scratch on device `dev` (current), looked up
+// once per device.  In host code the array's name is only a host-side
+// stand-in, never a device address.
+tsm_status static_scratch(int dev, void** out) {
+  if (dev < 0 || dev >= kStaticScratchDevices) return TSM_ERROR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (g_static_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, tsm_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(tsm_static_scratch)");
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return TSM_SUCCESS;
+}
+
+}  // namespace
+}  // namespace tsm
+
+extern "C" tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, int m, int k, const double* A,
+                                              int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc,
+                                              int accumulate) {
+  using namespace tsm;
+  tsm_status s = check_args(n, m, k, A, lda, B, ldb, C, ldc);
+  if (s != TSM_SUCCESS) return s;
+  int dev = 0;
+  DeviceState* st = nullptr;
+  if ((s = current_device(&dev, &st)) != TSM_SUCCESS) return s;
+  void* scratch = nullptr;
+  if ((s = static_scratch(dev, &scratch)) != TSM_SUCCESS) return s;
+
+  // Same variant and grid as tsm_gemm_tn_f64 would use.
+  const int idx = default_variant(n, m, k, A, lda, B, ldb);
+  if (idx < 0) return TSM_ERROR_UNSUPPORTED;
+  if ((s = prepare_variant(st, idx)) != TSM_SUCCESS) return s;
+  const Variant* v = variants()[idx];
+
+  PlainArgs p{};
+  p.A = A;
+  p.B = B;
+  p.C = C;
+  p.n = n;
+  p.m = m;
+  p.k = k;
+  p.lda = lda;
+  p.ldb = ldb;
+  p.ldc = ldc;
+  p.accumulate = accumulate ? 1 : 0;
+  const int64_t max_grid = static_cast<int64_t>(st->sms) * st->occupancy[idx];
+  int64_t grid = 1;
+  if (v->kind == kKindBulk) {
+    p.rows_main = ((m % 2 == 0) && (k % 2 == 0)) ? n : (n & ~int64_t(1));
+    p.num_chunks = (p.rows_main + v->rows - 1) / v->rows;
+    grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, max_grid));
+  } else {
+    p.rows_main = n;
+    p.num_chunks = 0;
+    const int tiles = (v->wa / v->ta) * (v->wb / v->tb);
+    const int64_t row_groups = v->threads / tiles;
+    grid = std::max<int64_t>(1, std::min<int64_t>((n + row_groups - 1) / row_groups, max_grid));
+  }
+  const size_t need = kWsHeader + static_cast<size_t>(grid) * m * k * sizeof(double);
+  if (need > kStaticScratchBytes) return TSM_ERROR_WORKSPACE;
+
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  p.counter = reinterpret_cast<unsigned*>(base);
+  p.error = reinterpret_cast<unsigned*>(base) + 1;
+  p.partials = reinterpret_cast<double*>(base + kWsHeader);
+
+  cudaStream_t cs = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(unsigned), cs);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(static scratch counter)");
+  void* args[] = {&p};
+  e = cudaLaunchKernel(v->kernel, dim3(static_cast<unsigned>(grid)), dim3(v->threads), args, v->smem, cs);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernel");
+  return TSM_SUCCESS;
+}
