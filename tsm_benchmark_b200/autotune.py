@@ -34,11 +34,24 @@ BUCKETS = [(0, 1 << 15), (1 << 18, 1 << 20), (1 << 23, 1 << 26)]
 MAX_BYTES = 24 << 30  # per operand pair while tuning
 
 
+def _cap(w: int) -> int:
+    c = 1
+    while c < w:
+        c *= 2
+    return c
+
+
 def candidates(variants: list[dict], m: int, k: int) -> list[dict]:
+    """Variants that accept (m, k): every exact one, and the capacity ones
+    no more than twice the smallest capacity per side (larger ones only add
+    masked work)."""
     out = []
+    cm, ck = _cap(m), _cap(k)
     for v in variants:
-        fits = (m == v["wa"] and k == v["wb"]) if v["exact"] else (m <= v["wa"] and k <= v["wb"])
-        if fits:
+        if v["exact"]:
+            if m == v["wa"] and k == v["wb"]:
+                out.append(v)
+        elif m <= v["wa"] <= 2 * cm and k <= v["wb"] <= 2 * ck:
             out.append(v)
     return out
 

@@ -61,13 +61,62 @@ struct TileShape {
 
 namespace detail {
 
+// Undoes the chunk rotation of load_row_seg on a thread's register tile:
+// after loading with rotation `rot`, register pair q of a TW-wide segment
+// holds the segment's 16-byte chunk (q + rot) mod TW/2.  Rotating the pairs
+// right by `rot` (log2(TW/2) conditional stages with compile-time indices)
+// puts chunk c back in pair c, so that lanes with different rotations can
+// then be summed register by register.
+template <int TA, int TB>
+__device__ __forceinline__ void unrotate_tile(double (&acc)[TA][TB], int rotA, int rotB) {
+  if constexpr (TA >= 4 && (TA & (TA - 1)) == 0) {
+    constexpr int N = TA / 2;
+#pragma unroll
+    for (int b = 1; b < N; b <<= 1) {
+      if (rotA & b) {
+        double tmp[TA][TB];
+#pragma unroll
+        for (int c = 0; c < N; ++c)
+#pragma unroll
+          for (int e = 0; e < 2; ++e)
+#pragma unroll
+            for (int j = 0; j < TB; ++j) tmp[2 * c + e][j] = acc[2 * ((c - b + N) % N) + e][j];
+#pragma unroll
+        for (int i = 0; i < TA; ++i)
+#pragma unroll
+          for (int j = 0; j < TB; ++j) acc[i][j] = tmp[i][j];
+      }
+    }
+  }
+  if constexpr (TB >= 4 && (TB & (TB - 1)) == 0) {
+    constexpr int N = TB / 2;
+#pragma unroll
+    for (int b = 1; b < N; b <<= 1) {
+      if (rotB & b) {
+        double tmp[TA][TB];
+#pragma unroll
+        for (int i = 0; i < TA; ++i)
+#pragma unroll
+          for (int c = 0; c < N; ++c)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) tmp[i][2 * c + e] = acc[i][2 * ((c - b + N) % N) + e];
+#pragma unroll
+        for (int i = 0; i < TA; ++i)
+#pragma unroll
+          for (int j = 0; j < TB; ++j) acc[i][j] = tmp[i][j];
+      }
+    }
+  }
+}
+
 // Sums the per-thread tiles of one CTA into `red`, then into this CTA's slot
 // of the workspace; the last CTA then writes C.  `red` must hold
 // slots * m * k doubles.  Called by all threads of the CTA (nthreads), of
 // which the first `cthreads` carry tiles.
 template <int TA, int TB, int NT, bool EXACT, int WA, int WB>
 __device__ __forceinline__ void finish_tiles(const PlainArgs& p, double (&acc)[TA][TB], int t, int cthreads,
-                                             int nthreads, double* red, unsigned* s_is_last) {
+                                             int nthreads, double* red, unsigned* s_is_last, int rotA = 0,
+                                             int rotB = 0) {
   const int m = EXACT ? WA : p.m;
   const int k = EXACT ? WB : p.k;
   const int mk = m * k;
@@ -75,6 +124,7 @@ __device__ __forceinline__ void finish_tiles(const PlainArgs& p, double (&acc)[T
   const int tile = t % NT;
   const int ta = tile % (WA / TA), tb = tile / (WA / TA);
   const bool carrier = t < cthreads;
+  if (carrier) unrotate_tile<TA, TB>(acc, rotA, rotB);
 
   // 1. Warp level: lanes that share a tile differ by multiples of NT.
   if (carrier && NT < 32) {
@@ -142,12 +192,19 @@ __device__ __forceinline__ void outer_fma(double (&acc)[TA][TB], const double (&
 
 // Loads W consecutive doubles from shared memory (16-byte vector loads where
 // the layout allows) or, in capacity mode, up to `valid` of them (rest = 0).
+// With vector loads, chunk c of the segment goes to register pair
+// (c - rot) mod W/2: threads whose rows share shared-memory banks then read
+// different banks in the same instruction (the rows of a warp are a whole
+// number of 128-byte bank rows apart for row pitches of 64, 128, 256 and
+// 512 bytes).  The accumulators follow the registers, so the rotation is
+// undone once, on the finished tile (unrotate_tile).
 template <int W, bool VEC>
-__device__ __forceinline__ void load_row_seg(double (&v)[W], const double* src, int valid) {
+__device__ __forceinline__ void load_row_seg(double (&v)[W], const double* src, int valid, int rot = 0) {
   if constexpr (VEC) {
+    static_assert(((W / 2) & (W / 2 - 1)) == 0, "vector segments hold a power-of-two number of 16-byte chunks");
 #pragma unroll
     for (int i = 0; i < W / 2; ++i) {
-      const double2 x = reinterpret_cast<const double2*>(src)[i];
+      const double2 x = reinterpret_cast<const double2*>(src)[(i + rot) & (W / 2 - 1)];
       v[2 * i] = x.x;
       v[2 * i + 1] = x.y;
     }
@@ -180,6 +237,19 @@ struct BulkKernel {
   static constexpr size_t SMEM_BYTES = BAR_OFFSET + 2 * STAGES * sizeof(uint64_t) + 16;
   static constexpr bool VEC_A = EXACT && TA % 2 == 0 && WA % 2 == 0;
   static constexpr bool VEC_B = EXACT && TB % 2 == 0 && WB % 2 == 0;
+  // Chunk rotation (load_row_seg): a thread's rows r = rg + i*RG must all
+  // map to the same rotation, i.e. RG row pitches span whole multiples of
+  // 8 * (chunks per segment) 16-byte units.
+  static constexpr int NCH_A = TA / 2 > 0 ? TA / 2 : 1;
+  static constexpr int NCH_B = TB / 2 > 0 ? TB / 2 : 1;
+  static constexpr bool ROT_A = VEC_A && NCH_A > 1 && (RG * (WA / 2)) % (8 * NCH_A) == 0;
+  static constexpr bool ROT_B = VEC_B && NCH_B > 1 && (RG * (WB / 2)) % (8 * NCH_B) == 0;
+  // Rotation of a thread whose first row in a stage is rg and whose segment
+  // starts at column col: spreads the rows and column segments of one warp
+  // over the eight 16-byte bank groups.
+  __device__ static int rotation(int rg, int col, int width, int nch) {
+    return ((rg * (width / 2) + col / 2) / 8) & (nch - 1);
+  }
 };
 
 template <int WA, int WB, int TA, int TB, int CW, int STAGES, int RS, int UNROLL, bool EXACT>
@@ -250,6 +320,8 @@ __global__ void __launch_bounds__(BulkKernel<WA, WB, TA, TB, CW, STAGES, RS, UNR
     const int rg = t / S::NT;
     const int colA = ta * TA, colB = tb * TB;
     const int validA = m - colA, validB = k - colB;
+    const int rotA = K::ROT_A ? K::rotation(rg, colA, WA, K::NCH_A) : 0;
+    const int rotB = K::ROT_B ? K::rotation(rg, colB, WB, K::NCH_B) : 0;
     int64_t it = 0;
     for (int64_t c = blockIdx.x; c < p.num_chunks; c += G, ++it) {
       const int s = static_cast<int>(it % STAGES);
@@ -267,15 +339,15 @@ __global__ void __launch_bounds__(BulkKernel<WA, WB, TA, TB, CW, STAGES, RS, UNR
 #pragma unroll UNROLL
         for (int r = rg; r < RS; r += K::RG) {
           double a[TA], b[TB];
-          detail::load_row_seg<TA, K::VEC_A>(a, sa + r * m, validA);
-          detail::load_row_seg<TB, K::VEC_B>(b, sb + r * k, validB);
+          detail::load_row_seg<TA, K::VEC_A>(a, sa + r * m, validA, rotA);
+          detail::load_row_seg<TB, K::VEC_B>(b, sb + r * k, validB, rotB);
           detail::outer_fma<TA, TB>(acc, a, b);
         }
       } else {
         for (int r = rg; r < rows; r += K::RG) {
           double a[TA], b[TB];
-          detail::load_row_seg<TA, K::VEC_A>(a, sa + r * m, validA);
-          detail::load_row_seg<TB, K::VEC_B>(b, sb + r * k, validB);
+          detail::load_row_seg<TA, K::VEC_A>(a, sa + r * m, validA, rotA);
+          detail::load_row_seg<TB, K::VEC_B>(b, sb + r * k, validB, rotB);
           detail::outer_fma<TA, TB>(acc, a, b);
         }
       }
@@ -296,8 +368,15 @@ __global__ void __launch_bounds__(BulkKernel<WA, WB, TA, TB, CW, STAGES, RS, UNR
   }
   __syncthreads();
 
+  int rotA = 0, rotB = 0;
+  if (warp < CW) {
+    const int tile = t % S::NT;
+    const int rg = t / S::NT;
+    rotA = K::ROT_A ? K::rotation(rg, (tile % S::QA) * TA, WA, K::NCH_A) : 0;
+    rotB = K::ROT_B ? K::rotation(rg, (tile / S::QA) * TB, WB, K::NCH_B) : 0;
+  }
   detail::finish_tiles<TA, TB, S::NT, EXACT, WA, WB>(p, acc, t, K::CT, K::THREADS,
-                                                       reinterpret_cast<double*>(smem), s_is_last);
+                                                       reinterpret_cast<double*>(smem), s_is_last, rotA, rotB);
 }
 
 // --------------------------------------------------------------------------
