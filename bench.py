@@ -306,7 +306,7 @@ def main() -> int:
     dev_err = int(bits.value)
 
     # ---------------- the dominant kernel's roofline (the only kernel here)
-    vidx = lib.tsm_gemm_tn_default_variant(HEAD_N, HEAD_M, HEAD_K, A.data_ptr(), HEAD_M, B.data_ptr(), HEAD_K)
+    vidx = lib.tsm_gemm_tn_default_variant(0, HEAD_N, HEAD_M, HEAD_K, A.data_ptr(), HEAD_M, B.data_ptr(), HEAD_K)
     vname = tsm.variants()[vidx]["name"] if vidx >= 0 else None
     # time the kernel alone (no reduction step) for the roofline figure
     kev0 = torch.cuda.Event(enable_timing=True)
@@ -342,7 +342,7 @@ def main() -> int:
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / args.sweep_steps
             gbs = algo_bytes(n, m, k) / (ms * 1e-3) / 1e9
-            vi = lib.tsm_gemm_tn_default_variant(n, m, k, a.data_ptr(), m, b.data_ptr(), k)
+            vi = lib.tsm_gemm_tn_default_variant(0, n, m, k, a.data_ptr(), m, b.data_ptr(), k)
             by_width.append({"n": n, "m": m, "k": k, "ms": round(ms, 4), "GB/s": round(gbs, 1),
                              "frac_hbm": round(gbs / peaks["hbm_gbs"], 4),
                              "GFLOP/s": round(2.0 * n * m * k / (ms * 1e-3) / 1e9, 1),

@@ -83,13 +83,30 @@ tsm_status tsm_gemm_tn_f64_variant(tsm_stream_t stream, int64_t n, int m, int k,
                                    const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
                                    void* workspace, size_t workspace_bytes, int variant);
 
-/* Index of the variant tsm_gemm_tn_f64 would run for this request, or -1. */
-int tsm_gemm_tn_default_variant(int64_t n, int m, int k, const void* A, int64_t lda, const void* B,
+/* C = A^T B or C += A^T B with FP32 storage (A, B, C float).  Each thread
+ * accumulates in FP32 over its rows; every sum across threads and CTAs is
+ * FP64, then rounded once to FP32.  The FP32 forward of the autograd form
+ * (torch.autograd.Function over the C ABI).  Same workspace as the FP64 call. */
+tsm_status tsm_gemm_tn_f32(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                           const float* B, int64_t ldb, float* C, int64_t ldc, int accumulate, void* workspace,
+                           size_t workspace_bytes);
+tsm_status tsm_gemm_tn_f32_variant(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                                   const float* B, int64_t ldb, float* C, int64_t ldc, int accumulate,
+                                   void* workspace, size_t workspace_bytes, int variant);
+
+/* Element types of the plain entry points. */
+#define TSM_F64 0
+#define TSM_F32 1
+
+/* Index of the variant tsm_gemm_tn_f64 (dtype TSM_F64) or tsm_gemm_tn_f32
+ * (TSM_F32) would run for this request, or -1. */
+int tsm_gemm_tn_default_variant(int dtype, int64_t n, int m, int k, const void* A, int64_t lda, const void* B,
                                 int64_t ldb);
 
 typedef struct tsm_variant_info {
   char name[64];
   int kind;    /* 0 = TMA bulk pipeline, 1 = direct loads */
+  int dtype;   /* TSM_F64 or TSM_F32 */
   int wa, wb;  /* widths (exact) or width capacities */
   int ta, tb;  /* per-thread tile of C */
   int exact;   /* 1: only m == wa, k == wb */
@@ -125,6 +142,78 @@ tsm_status tsm_workspace_check(tsm_stream_t stream, void* workspace, unsigned* b
  * before any stream capture.  Device error bits are not reported. */
 tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
                                    const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate);
+
+/* Tall-skinny times small (TSMM): Y (n x q) = X (n x p) * W (beta = 0) or
+ * Y += X * W (beta = 1), FP64 or FP32, 1 <= p, q <= 64.  W is read as
+ * W[a][b] = W[a * w_row + b * w_col], so a row-major p x q matrix is
+ * (w_row, w_col) = (q, 1) and the transpose of a row-major q x p matrix is
+ * (1, p).  No counterpart in the reference (it has no backward); this is the
+ * product the backward of C = A^T B needs, and the second half of block
+ * orthogonalisation B - A (A^T B).  Each output is one fixed-order sum over
+ * p (deterministic).  Workspace: at least 256 bytes (the device error word);
+ * the plain calls' workspace serves. */
+tsm_status tsm_tsmm_f64(tsm_stream_t stream, int64_t n, int p, int q, const double* X, int64_t ldx, const double* W,
+                        int64_t w_row, int64_t w_col, double* Y, int64_t ldy, int beta, void* workspace,
+                        size_t workspace_bytes);
+tsm_status tsm_tsmm_f32(tsm_stream_t stream, int64_t n, int p, int q, const float* X, int64_t ldx, const float* W,
+                        int64_t w_row, int64_t w_col, float* Y, int64_t ldy, int beta, void* workspace,
+                        size_t workspace_bytes);
+
+/* Backward of C = A^T B for a loss L(C): given dC = dL/dC (m x k), writes
+ * dA = B * dC^T (n x m) and dB = A * dC (n x k) in ONE launch (either output
+ * may be NULL to skip it); beta = 1 adds into dA / dB instead.  Reads A and B
+ * once each and writes dA and dB once each: 2x the bytes of the forward.
+ * No counterpart in the reference (the differentiation form). */
+tsm_status tsm_gemm_tn_backward_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                                    const double* B, int64_t ldb, const double* dC, int64_t lddc, double* dA,
+                                    int64_t ldda, double* dB, int64_t lddb, int beta, void* workspace,
+                                    size_t workspace_bytes);
+tsm_status tsm_gemm_tn_backward_f32(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                                    const float* B, int64_t ldb, const float* dC, int64_t lddc, float* dA,
+                                    int64_t ldda, float* dB, int64_t lddb, int beta, void* workspace,
+                                    size_t workspace_bytes);
+
+/* ---- Batched products: many C_p = A_p^T B_p (+ C_p) in one launch. ----
+ * No counterpart in the reference (it submits one kernel per product; the
+ * batching form).  Widths m, k in {4, 8, 16, 32}; A_p, B_p contiguous
+ * (lda = m, ldb = k) and 16-byte aligned; any n_p >= 0. */
+typedef struct tsm_batched_problem_f64 {
+  const double* A;
+  const double* B;
+  double* C;
+  int64_t n;
+  int m;
+  int k;
+  int64_t ldc;
+  int accumulate;
+} tsm_batched_problem_f64;
+
+/* Host handle of a plan whose tables live in caller-owned device memory. */
+typedef struct tsm_batched_plan {
+  void* device;
+  size_t bytes;
+  int count;
+  int segments;
+  int grid;
+  int reserved;
+} tsm_batched_plan;
+
+/* Device bytes the plan for these problems needs on the current device
+ * (0 if a problem is invalid or unsupported). */
+size_t tsm_batched_plan_size_f64(int count, const tsm_batched_problem_f64* problems);
+
+/* Builds the schedule on the host -- the problems' rows concatenated and cut
+ * into one equal byte range per SM, each a list of row segments -- and copies
+ * it into `device_buffer` (synchronising `stream`).  Pointers and sizes are
+ * baked into the plan: re-initialise it when they change. */
+tsm_status tsm_batched_plan_init_f64(tsm_stream_t stream, int count, const tsm_batched_problem_f64* problems,
+                                     void* device_buffer, size_t device_bytes, tsm_batched_plan* plan);
+
+/* Runs every product of the plan in ONE persistent launch (capturable in a
+ * CUDA graph; the plan's first execution, or any other call, must happen
+ * before capture so that the kernel is loaded).  Deterministic for a given
+ * plan.  Concurrent executions of one plan race on its counters. */
+tsm_status tsm_gemm_tn_batched_f64(tsm_stream_t stream, const tsm_batched_plan* plan);
 
 /* Benchmark-input generator: x[i] = 2u - 1 in [-1, 1), u the top 53 bits of
  * SplitMix64 at counter (stream_id * 2^40 + i + 1) under `seed`.  The same

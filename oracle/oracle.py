@@ -76,8 +76,15 @@ def _p(a: np.ndarray):
 
 
 def _rows(x: np.ndarray) -> tuple[int, int, int]:
-    assert x.ndim == 2 and x.strides[1] == x.itemsize
-    return x.shape[0], x.shape[1], (x.strides[0] // x.itemsize if x.shape[0] > 1 else x.shape[1])
+    assert x.ndim == 2
+    if x.shape[0] <= 1 or x.shape[1] <= 1:
+        # strides of empty, single-row or single-column arrays carry no layout
+        assert x.flags.c_contiguous or x.shape[1] <= 1 or x.shape[0] <= 1
+        if x.shape[1] <= 1 and x.shape[0] > 1:
+            return x.shape[0], x.shape[1], x.strides[0] // x.itemsize
+        return x.shape[0], x.shape[1], max(1, x.shape[1])
+    assert x.strides[1] == x.itemsize
+    return x.shape[0], x.shape[1], x.strides[0] // x.itemsize
 
 
 def naive(A: np.ndarray, B: np.ndarray) -> np.ndarray:

@@ -112,6 +112,8 @@ def test_every_applicable_variant(gpu, oracle_mod):
         cases[(m, k)] = oracle_mod.operands(3001, m, k, 11 + m + k)
     ran = 0
     for v in variants():
+        if v["dtype"] != "f64":
+            continue
         for (m, k), (A, B) in cases.items():
             fits = (m == v["wa"] and k == v["wb"]) if v["exact"] else (m <= v["wa"] and k <= v["wb"])
             if not fits:
@@ -152,7 +154,9 @@ def test_argument_errors(gpu):
     with pytest.raises(TsmError):
         tsmttsm(A, A)
     with pytest.raises(TypeError):
-        tsmttsm(A.float(), A.float())
+        tsmttsm(A.half(), A.half())
+    with pytest.raises(TypeError):
+        tsmttsm(A, A.float())
     lib = _capi.load()
     A = torch.zeros((10, 8), dtype=torch.float64, device=gpu)
     C = torch.zeros((8, 8), dtype=torch.float64, device=gpu)
@@ -192,3 +196,28 @@ def test_full_size_properties(gpu, m, k):
     assert abs(float(C.sum()) - chk) <= 4 * bound * np.sqrt(m * k)
     del A, B
     torch.cuda.empty_cache()
+
+
+F32_SHAPES = [(1, 1), (2, 2), (3, 5), (4, 4), (8, 8), (16, 16), (32, 32), (64, 64), (4, 32), (7, 13)]
+
+
+@pytest.mark.parametrize("m,k", F32_SHAPES)
+def test_parity_fp32_storage(gpu, oracle_mod, m, k):
+    """FP32 storage: per-thread FP32 accumulation, FP64 reductions, one
+    rounding to FP32.  Checked against the oracle's FP64 product of the FP32
+    values with a bound for FP32 accumulation over the rows one thread sums:
+    ||C - C_ref||_F <= 2^-24 (rows per thread + 2) ||A||_F ||B||_F."""
+    from tsm_benchmark_b200 import tsmttsm, variants
+    for n in (0, 1, 3, 4099, 100003):
+        A, B = oracle_mod.operands(n, m, k, seed=77 + n + m * k)
+        A32, B32 = A.astype(np.float32), B.astype(np.float32)
+        C = tsmttsm(to_dev(A32, gpu), to_dev(B32, gpu))
+        assert C.dtype == torch.float32
+        ref = oracle_mod.naive(A32, B32)
+        got = C.cpu().numpy().astype(np.float64)
+        err = np.linalg.norm(got - ref)
+        per_thread = max(1, n // (148 * 8)) + 2
+        bound = 2.0**-24 * per_thread * np.linalg.norm(A32.astype(np.float64)) * np.linalg.norm(B32.astype(np.float64))
+        assert err <= bound + 1e-30, (n, m, k, err, bound)
+    names = [v for v in variants() if v["dtype"] == "f32"]
+    assert names

@@ -6,6 +6,9 @@ side: ctypes bindings, torch-tensor entry points, the variant generator and
 the autotuner.
 """
 from ._capi import TsmError, TsmLibraryError, variants  # noqa: F401
-from .api import default_variant, fill_uniform, tsmttsm, workspace_status  # noqa: F401
+from .api import (default_variant, fill_uniform, tsmm, tsmttsm, tsmttsm_backward,  # noqa: F401
+                  workspace_status)
+from .autograd import TSMTTSMFunction, gram_tn  # noqa: F401
+from .batched import BatchedTSMTTSM  # noqa: F401
 
 __version__ = "0.1.0"

@@ -18,6 +18,8 @@ c_size_t = ctypes.c_size_t
 c_void_p = ctypes.c_void_p
 c_uint64 = ctypes.c_uint64
 
+DTYPE = {"f64": 0, "f32": 1}
+
 STATUS = {
     0: "TSM_SUCCESS",
     1: "TSM_ERROR_INVALID_VALUE",
@@ -44,12 +46,23 @@ class VariantInfo(ctypes.Structure):
     _fields_ = [
         ("name", ctypes.c_char * 64),
         ("kind", c_int),
+        ("dtype", c_int),
         ("wa", c_int), ("wb", c_int),
         ("ta", c_int), ("tb", c_int),
         ("exact", c_int),
         ("threads", c_int), ("stages", c_int), ("rows", c_int), ("unroll", c_int),
         ("smem_bytes", c_size_t),
     ]
+
+
+class BatchedProblem(ctypes.Structure):
+    _fields_ = [("A", c_void_p), ("B", c_void_p), ("C", c_void_p), ("n", c_int64), ("m", c_int), ("k", c_int),
+                ("ldc", c_int64), ("accumulate", c_int)]
+
+
+class BatchedPlan(ctypes.Structure):
+    _fields_ = [("device", c_void_p), ("bytes", c_size_t), ("count", c_int), ("segments", c_int),
+                ("grid", c_int), ("reserved", c_int)]
 
 
 # Every function declared in include/tsm.h: name -> (restype, argtypes).
@@ -62,11 +75,29 @@ SIGNATURES = {
                                 c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_f64_variant": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int, c_void_p, c_size_t, c_int]),
-    "tsm_gemm_tn_default_variant": (c_int, [c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64]),
+    "tsm_gemm_tn_f32": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                c_void_p, c_int64, c_int, c_void_p, c_size_t]),
+    "tsm_gemm_tn_f32_variant": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                        c_void_p, c_int64, c_int, c_void_p, c_size_t, c_int]),
+    "tsm_gemm_tn_default_variant": (c_int, [c_int, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64]),
     "tsm_variant_count": (c_int, []),
     "tsm_variant_get_info": (c_int, [c_int, ctypes.POINTER(VariantInfo)]),
     "tsm_workspace_check": (c_int, [c_void_p, c_void_p, ctypes.POINTER(ctypes.c_uint)]),
     "tsm_fill_uniform_f64": (c_int, [c_void_p, c_void_p, c_int64, c_uint64, c_uint64]),
+    "tsm_tsmm_f64": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_int64,
+                             c_void_p, c_int64, c_int, c_void_p, c_size_t]),
+    "tsm_tsmm_f32": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_int64,
+                             c_void_p, c_int64, c_int, c_void_p, c_size_t]),
+    "tsm_gemm_tn_backward_f64": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                         c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_int,
+                                         c_void_p, c_size_t]),
+    "tsm_gemm_tn_backward_f32": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                         c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_int,
+                                         c_void_p, c_size_t]),
+    "tsm_batched_plan_size_f64": (c_size_t, [c_int, ctypes.POINTER(BatchedProblem)]),
+    "tsm_batched_plan_init_f64": (c_int, [c_void_p, c_int, ctypes.POINTER(BatchedProblem), c_void_p, c_size_t,
+                                          ctypes.POINTER(BatchedPlan)]),
+    "tsm_gemm_tn_batched_f64": (c_int, [c_void_p, ctypes.POINTER(BatchedPlan)]),
     "tsm_gemm_tn_f64_noalloc": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int]),
 }
@@ -118,6 +149,7 @@ def variants() -> list[dict]:
         info = VariantInfo()
         check(lib.tsm_variant_get_info(i, ctypes.byref(info)), "tsm_variant_get_info")
         out.append(dict(index=i, name=info.name.decode(), kind="bulk" if info.kind == 0 else "direct",
+                        dtype="f64" if info.dtype == 0 else "f32",
                         wa=info.wa, wb=info.wb, ta=info.ta, tb=info.tb, exact=bool(info.exact),
                         threads=info.threads, stages=info.stages, rows=info.rows, unroll=info.unroll,
                         smem_bytes=info.smem_bytes))

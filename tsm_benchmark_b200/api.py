@@ -41,24 +41,33 @@ def _check_operand(x: torch.Tensor, name: str, dtype: torch.dtype) -> None:
         raise TypeError(f"{name} must be {dtype}, got {x.dtype}")
     if x.dim() != 2:
         raise ValueError(f"{name} must be 2-D, got shape {tuple(x.shape)}")
-    if x.shape[1] > 1 and x.stride(1) != 1:
+    if x.shape[0] > 0 and x.shape[1] > 1 and x.stride(1) != 1:
         raise ValueError(f"{name} must have unit column stride (row-major rows)")
 
 
 def _ld(x: torch.Tensor) -> int:
-    return max(int(x.stride(0)), int(x.shape[1])) if x.shape[0] > 1 else int(x.shape[1])
+    """Leading dimension (elements between rows); strides of empty or
+    single-row tensors carry no layout, so those report their width."""
+    return max(int(x.stride(0)), int(x.shape[1])) if x.shape[0] > 1 else max(1, int(x.shape[1]))
+
+
+_PLAIN = {torch.float64: ("tsm_gemm_tn_f64_variant", 0), torch.float32: ("tsm_gemm_tn_f32_variant", 1)}
 
 
 def tsmttsm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, accumulate: bool = False,
             variant: int = -1, stream: torch.cuda.Stream | None = None) -> torch.Tensor:
-    """C = A^T B (or C += A^T B with ``accumulate=True``) in FP64.
+    """C = A^T B (or C += A^T B with ``accumulate=True``), FP64 or FP32.
 
-    The Python face of ``tsm_gemm_tn_f64`` (the reference's
-    ``tsmttsm*<double, M, ...>(q, K, A, B, C)``, tsmttsm.hh:15-586, which
-    always accumulates).  Returns C; allocates it (m x k) when not given.
+    The Python face of ``tsm_gemm_tn_f64`` / ``tsm_gemm_tn_f32`` (the
+    reference's ``tsmttsm*<double, M, ...>(q, K, A, B, C)``,
+    tsmttsm.hh:15-586, which always accumulates).  A, B and C share one
+    dtype.  Returns C; allocates it (m x k) when not given.
     """
-    _check_operand(A, "A", torch.float64)
-    _check_operand(B, "B", torch.float64)
+    if A.dtype not in _PLAIN:
+        raise TypeError(f"A must be float64 or float32, got {A.dtype}")
+    fn_name, _ = _PLAIN[A.dtype]
+    _check_operand(A, "A", A.dtype)
+    _check_operand(B, "B", A.dtype)
     if A.shape[0] != B.shape[0]:
         raise ValueError(f"A and B must have the same number of rows, got {A.shape[0]} and {B.shape[0]}")
     if A.device != B.device:
@@ -68,9 +77,9 @@ def tsmttsm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, 
     if C is None:
         if accumulate:
             raise ValueError("accumulate=True needs an existing C")
-        C = torch.empty((m, k), dtype=torch.float64, device=A.device)
+        C = torch.empty((m, k), dtype=A.dtype, device=A.device)
     else:
-        _check_operand(C, "C", torch.float64)
+        _check_operand(C, "C", A.dtype)
         if tuple(C.shape) != (m, k):
             raise ValueError(f"C must be {m}x{k}, got {tuple(C.shape)}")
     lib = _capi.load()
@@ -80,16 +89,17 @@ def tsmttsm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, 
         if need == 0:
             _capi.check(1, "tsm_gemm_tn_workspace_size")
         ws = workspace(A.device, need, sh)
-        st = lib.tsm_gemm_tn_f64_variant(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
-                                         _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel(), int(variant))
-        _capi.check(st, "tsm_gemm_tn_f64")
+        st = getattr(lib, fn_name)(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
+                                   _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel(), int(variant))
+        _capi.check(st, fn_name)
     return C
 
 
 def default_variant(A: torch.Tensor, B: torch.Tensor) -> int:
     """Index of the variant tsmttsm() would run for these operands."""
     lib = _capi.load()
-    return lib.tsm_gemm_tn_default_variant(A.shape[0], A.shape[1], B.shape[1], A.data_ptr(), _ld(A),
+    dtype = _PLAIN[A.dtype][1] if A.dtype in _PLAIN else -1
+    return lib.tsm_gemm_tn_default_variant(dtype, A.shape[0], A.shape[1], B.shape[1], A.data_ptr(), _ld(A),
                                            B.data_ptr(), _ld(B))
 
 
@@ -121,3 +131,72 @@ def fill_uniform(x: torch.Tensor, seed: int, stream_id: int = 0, stream: torch.c
                                       seed & 0xFFFFFFFFFFFFFFFF, stream_id & 0xFFFFFFFFFFFFFFFF)
     _capi.check(st, "tsm_fill_uniform_f64")
     return x
+
+
+_TSMM = {torch.float64: "tsm_tsmm_f64", torch.float32: "tsm_tsmm_f32"}
+_BWD = {torch.float64: "tsm_gemm_tn_backward_f64", torch.float32: "tsm_gemm_tn_backward_f32"}
+
+
+def tsmm(X: torch.Tensor, W: torch.Tensor, Y: torch.Tensor | None = None, *, transpose_w: bool = False,
+         accumulate: bool = False, stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """Y = X @ W (or X @ W.T with ``transpose_w``), tall-skinny X (n x p),
+    small W; ``accumulate=True`` adds into Y.  ``tsm_tsmm_f64`` / ``_f32``."""
+    if X.dtype not in _TSMM:
+        raise TypeError(f"X must be float64 or float32, got {X.dtype}")
+    _check_operand(X, "X", X.dtype)
+    if not W.is_cuda or W.dtype != X.dtype or W.dim() != 2:
+        raise ValueError("W must be a 2-D CUDA tensor of X's dtype")
+    n, p = X.shape
+    if transpose_w:
+        q, pw = W.shape
+        w_row, w_col = W.stride(1), W.stride(0)
+    else:
+        pw, q = W.shape
+        w_row, w_col = W.stride(0), W.stride(1)
+    if pw != p:
+        raise ValueError(f"W must have {p} rows (after transposition), got {pw}")
+    if Y is None:
+        if accumulate:
+            raise ValueError("accumulate=True needs an existing Y")
+        Y = torch.empty((n, q), dtype=X.dtype, device=X.device)
+    else:
+        _check_operand(Y, "Y", X.dtype)
+        if tuple(Y.shape) != (n, q):
+            raise ValueError(f"Y must be {n}x{q}, got {tuple(Y.shape)}")
+    lib = _capi.load()
+    with torch.cuda.device(X.device):
+        sh = _stream_handle(X.device, stream)
+        ws = workspace(X.device, 256, sh)
+        st = getattr(lib, _TSMM[X.dtype])(sh, n, p, q, X.data_ptr(), _ld(X), W.data_ptr(), w_row, w_col,
+                                           Y.data_ptr(), _ld(Y), 1 if accumulate else 0, ws.data_ptr(), ws.numel())
+        _capi.check(st, _TSMM[X.dtype])
+    return Y
+
+
+def tsmttsm_backward(A: torch.Tensor, B: torch.Tensor, dC: torch.Tensor, *, need_dA: bool = True,
+                     need_dB: bool = True, stream: torch.cuda.Stream | None = None):
+    """(dA, dB) = (B @ dC.T, A @ dC) for C = A^T B, in one launch
+    (``tsm_gemm_tn_backward_*``); an output not needed is returned as None."""
+    if A.dtype not in _BWD:
+        raise TypeError(f"A must be float64 or float32, got {A.dtype}")
+    _check_operand(A, "A", A.dtype)
+    _check_operand(B, "B", A.dtype)
+    n, m = A.shape
+    k = B.shape[1]
+    if B.shape[0] != n:
+        raise ValueError("A and B must have the same number of rows")
+    if tuple(dC.shape) != (m, k) or dC.dtype != A.dtype or not dC.is_cuda:
+        raise ValueError(f"dC must be a {m}x{k} CUDA tensor of A's dtype")
+    dC = dC.contiguous()
+    dA = torch.empty((n, m), dtype=A.dtype, device=A.device) if need_dA else None
+    dB = torch.empty((n, k), dtype=A.dtype, device=A.device) if need_dB else None
+    lib = _capi.load()
+    with torch.cuda.device(A.device):
+        sh = _stream_handle(A.device, stream)
+        ws = workspace(A.device, 256, sh)
+        st = getattr(lib, _BWD[A.dtype])(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), dC.data_ptr(),
+                                          k, dA.data_ptr() if dA is not None else None, m,
+                                          dB.data_ptr() if dB is not None else None, k, 0, ws.data_ptr(),
+                                          ws.numel())
+        _capi.check(st, _BWD[A.dtype])
+    return dA, dB

@@ -65,16 +65,27 @@ class BulkVariant:
     rows: int = 0  # 0: sized for ~32 KB stages
     unroll: int = 1
     exact: bool = True
+    dtype: str = "f64"
+
+    @property
+    def esize(self) -> int:
+        return 8 if self.dtype == "f64" else 4
+
+    @property
+    def epc(self) -> int:  # elements per 16-byte chunk
+        return 16 // self.esize
 
     def resolved(self) -> "BulkVariant":
         if self.rows:
             return self
         rg = self.cw * 32 // self.num_tiles
-        rows = max(2, (32768 // (8 * (self.wa + self.wb))) // 2 * 2)
-        # Round to whole passes of the row groups, keeping chunks even.
+        e = self.epc
+        rows = max(e, (32768 // (self.esize * (self.wa + self.wb))) // e * e)
+        # Round to whole passes of the row groups, keeping every bulk copy a
+        # multiple of 16 bytes.
         if rows >= rg:
             rows = rows // rg * rg
-        rows = max(2, rows // 2 * 2)
+        rows = max(e, rows // e * e)
         return dataclasses.replace(self, rows=rows)
 
     @property
@@ -84,7 +95,8 @@ class BulkVariant:
     @property
     def name(self) -> str:
         v = self.resolved()
-        s = (f"bulk_{v.wa}x{v.wb}_t{v.ta}x{v.tb}_w{v.cw}_s{v.stages}"
+        kind = "bulk" if v.dtype == "f64" else "bulkf32"
+        s = (f"{kind}_{v.wa}x{v.wb}_t{v.ta}x{v.tb}_w{v.cw}_s{v.stages}"
              f"_r{v.rows}_u{v.unroll}")
         return s if v.exact else s + "_cap"
 
@@ -93,7 +105,7 @@ class BulkVariant:
         ct = v.cw * 32
         nt = v.num_tiles
         slots = v.cw if nt < 32 else ct // nt
-        ring = v.stages * v.rows * (v.wa + v.wb) * 8
+        ring = v.stages * v.rows * (v.wa + v.wb) * v.esize
         red = slots * v.wa * v.wb * 8
         data = max(ring, red)
         return (data + 127) // 128 * 128 + 2 * v.stages * 8 + 16
@@ -108,8 +120,10 @@ class BulkVariant:
             errs.append("tile count must be a power of two")
         if (v.cw * 32) % nt:
             errs.append("consumer threads must cover whole tiles")
-        if v.rows % 2:
-            errs.append("chunk rows must be even")
+        if v.rows % v.epc:
+            errs.append("chunk rows must keep bulk copies a multiple of 16 bytes")
+        if v.dtype not in ("f64", "f32"):
+            errs.append("dtype must be f64 or f32")
         rg = v.cw * 32 // max(nt, 1)
         if v.rows >= rg and (v.rows // rg) % v.unroll:
             errs.append("unroll must divide the rows per thread")
@@ -121,7 +135,8 @@ class BulkVariant:
 
     def emit(self) -> str:
         v = self.resolved()
-        return (f'TSM_BULK_VARIANT("{self.name}", {v.wa}, {v.wb}, {v.ta}, {v.tb}, '
+        ctype = "double" if v.dtype == "f64" else "float"
+        return (f'TSM_BULK_VARIANT("{self.name}", {ctype}, {v.wa}, {v.wb}, {v.ta}, {v.tb}, '
                 f'{v.cw}, {v.stages}, {v.rows}, {v.unroll}, '
                 f'{"true" if v.exact else "false"})')
 
@@ -136,6 +151,7 @@ class DirectVariant:
     tb: int
     threads: int = 256
     exact: bool = False
+    dtype: str = "f64"
 
     @property
     def num_tiles(self) -> int:
@@ -143,7 +159,8 @@ class DirectVariant:
 
     @property
     def name(self) -> str:
-        s = f"direct_{self.wa}x{self.wb}_t{self.ta}x{self.tb}_th{self.threads}"
+        kind = "direct" if self.dtype == "f64" else "directf32"
+        s = f"{kind}_{self.wa}x{self.wb}_t{self.ta}x{self.tb}_th{self.threads}"
         return s if self.exact else s + "_cap"
 
     def validate(self) -> list[str]:
@@ -160,7 +177,8 @@ class DirectVariant:
         return errs
 
     def emit(self) -> str:
-        return (f'TSM_DIRECT_VARIANT("{self.name}", {self.wa}, {self.wb}, {self.ta}, '
+        ctype = "double" if self.dtype == "f64" else "float"
+        return (f'TSM_DIRECT_VARIANT("{self.name}", {ctype}, {self.wa}, {self.wb}, {self.ta}, '
                 f'{self.tb}, {self.threads}, {"true" if self.exact else "false"})')
 
 
@@ -201,6 +219,16 @@ def default_variants() -> list:
     for wa in WIDTH_CAPS:
         for wb in WIDTH_CAPS:
             out.append(DirectVariant(wa, wb, default_tile(wa), default_tile(wb)))
+    # FP32 storage (FP32 per-thread accumulation, FP64 reductions): exact
+    # squares, then capacities, then direct loads, in the same order.
+    for w in WIDTH_CAPS:
+        out.append(BulkVariant(w, w, default_tile(w), default_tile(w), dtype="f32"))
+    for wa in WIDTH_CAPS:
+        for wb in WIDTH_CAPS:
+            out.append(BulkVariant(wa, wb, default_tile(wa), default_tile(wb), exact=False, dtype="f32"))
+    for wa in WIDTH_CAPS:
+        for wb in WIDTH_CAPS:
+            out.append(DirectVariant(wa, wb, default_tile(wa), default_tile(wb), dtype="f32"))
     return out
 
 
@@ -288,8 +316,8 @@ def compat_variant_for(vs: list, m: int, tm: int) -> str | None:
     """The exact bulk variant whose register tile is the reference's TM x TM
     for width m, else None (the library default is used)."""
     for v in vs:
-        if isinstance(v, BulkVariant) and v.exact and (v.wa, v.wb, v.ta, v.tb) == (m, m, tm, tm) \
-                and v.unroll == 1 and v.cw == 8 and v.stages == 6:
+        if isinstance(v, BulkVariant) and v.exact and v.dtype == "f64" \
+                and (v.wa, v.wb, v.ta, v.tb) == (m, m, tm, tm) and v.unroll == 1 and v.cw == 8 and v.stages == 6:
             return v.name
     return None
 

@@ -7,25 +7,38 @@ namespace tsm {
 
 extern const Variant kGenPart3[];
 const Variant kGenPart3[] = {
-    TSM_BULK_VARIANT("bulk_1x64_t1x8_w8_s6_r32_u1", 1, 64, 1, 8, 8, 6, 32, 1, true),
-    TSM_BULK_VARIANT("bulk_4x32_t4x8_w8_s6_r64_u1", 4, 32, 4, 8, 8, 6, 64, 1, true),
-    TSM_BULK_VARIANT("bulk_16x4_t8x4_w8_s6_r128_u1", 16, 4, 8, 4, 8, 6, 128, 1, true),
-    TSM_BULK_VARIANT("bulk_32x16_t8x8_w8_s6_r64_u1", 32, 16, 8, 8, 8, 6, 64, 1, true),
-    TSM_BULK_VARIANT("bulk_1x2_t1x2_w8_s6_r1280_u1_cap", 1, 2, 1, 2, 8, 6, 1280, 1, false),
-    TSM_BULK_VARIANT("bulk_2x4_t2x4_w8_s6_r512_u1_cap", 2, 4, 2, 4, 8, 6, 512, 1, false),
-    TSM_BULK_VARIANT("bulk_4x8_t4x4_w8_s6_r256_u1_cap", 4, 8, 4, 4, 8, 6, 256, 1, false),
-    TSM_BULK_VARIANT("bulk_8x16_t4x8_w8_s6_r128_u1_cap", 8, 16, 4, 8, 8, 6, 128, 1, false),
-    TSM_BULK_VARIANT("bulk_16x32_t8x8_w8_s6_r64_u1_cap", 16, 32, 8, 8, 8, 6, 64, 1, false),
-    TSM_BULK_VARIANT("bulk_32x64_t8x8_w8_s6_r40_u1_cap", 32, 64, 8, 8, 8, 6, 40, 1, false),
-    TSM_DIRECT_VARIANT("direct_1x1_t1x1_th256_cap", 1, 1, 1, 1, 256, false),
-    TSM_DIRECT_VARIANT("direct_2x2_t2x2_th256_cap", 2, 2, 2, 2, 256, false),
-    TSM_DIRECT_VARIANT("direct_4x4_t4x4_th256_cap", 4, 4, 4, 4, 256, false),
-    TSM_DIRECT_VARIANT("direct_8x8_t4x4_th256_cap", 8, 8, 4, 4, 256, false),
-    TSM_DIRECT_VARIANT("direct_16x16_t8x8_th256_cap", 16, 16, 8, 8, 256, false),
-    TSM_DIRECT_VARIANT("direct_32x32_t8x8_th256_cap", 32, 32, 8, 8, 256, false),
-    TSM_DIRECT_VARIANT("direct_64x64_t8x8_th256_cap", 64, 64, 8, 8, 256, false),
+    TSM_BULK_VARIANT("bulk_1x64_t1x8_w8_s6_r32_u1", double, 1, 64, 1, 8, 8, 6, 32, 1, true),
+    TSM_BULK_VARIANT("bulk_4x32_t4x8_w8_s6_r64_u1", double, 4, 32, 4, 8, 8, 6, 64, 1, true),
+    TSM_BULK_VARIANT("bulk_16x4_t8x4_w8_s6_r128_u1", double, 16, 4, 8, 4, 8, 6, 128, 1, true),
+    TSM_BULK_VARIANT("bulk_32x16_t8x8_w8_s6_r64_u1", double, 32, 16, 8, 8, 8, 6, 64, 1, true),
+    TSM_BULK_VARIANT("bulk_1x2_t1x2_w8_s6_r1280_u1_cap", double, 1, 2, 1, 2, 8, 6, 1280, 1, false),
+    TSM_BULK_VARIANT("bulk_2x4_t2x4_w8_s6_r512_u1_cap", double, 2, 4, 2, 4, 8, 6, 512, 1, false),
+    TSM_BULK_VARIANT("bulk_4x8_t4x4_w8_s6_r256_u1_cap", double, 4, 8, 4, 4, 8, 6, 256, 1, false),
+    TSM_BULK_VARIANT("bulk_8x16_t4x8_w8_s6_r128_u1_cap", double, 8, 16, 4, 8, 8, 6, 128, 1, false),
+    TSM_BULK_VARIANT("bulk_16x32_t8x8_w8_s6_r64_u1_cap", double, 16, 32, 8, 8, 8, 6, 64, 1, false),
+    TSM_BULK_VARIANT("bulk_32x64_t8x8_w8_s6_r40_u1_cap", double, 32, 64, 8, 8, 8, 6, 40, 1, false),
+    TSM_DIRECT_VARIANT("direct_1x1_t1x1_th256_cap", double, 1, 1, 1, 1, 256, false),
+    TSM_DIRECT_VARIANT("direct_2x2_t2x2_th256_cap", double, 2, 2, 2, 2, 256, false),
+    TSM_DIRECT_VARIANT("direct_4x4_t4x4_th256_cap", double, 4, 4, 4, 4, 256, false),
+    TSM_DIRECT_VARIANT("direct_8x8_t4x4_th256_cap", double, 8, 8, 4, 4, 256, false),
+    TSM_DIRECT_VARIANT("direct_16x16_t8x8_th256_cap", double, 16, 16, 8, 8, 256, false),
+    TSM_DIRECT_VARIANT("direct_32x32_t8x8_th256_cap", double, 32, 32, 8, 8, 256, false),
+    TSM_DIRECT_VARIANT("direct_64x64_t8x8_th256_cap", double, 64, 64, 8, 8, 256, false),
+    TSM_BULK_VARIANT("bulkf32_1x1_t1x1_w8_s6_r4096_u1_cap", float, 1, 1, 1, 1, 8, 6, 4096, 1, false),
+    TSM_BULK_VARIANT("bulkf32_2x2_t2x2_w8_s6_r2048_u1_cap", float, 2, 2, 2, 2, 8, 6, 2048, 1, false),
+    TSM_BULK_VARIANT("bulkf32_4x4_t4x4_w8_s6_r1024_u1_cap", float, 4, 4, 4, 4, 8, 6, 1024, 1, false),
+    TSM_BULK_VARIANT("bulkf32_8x8_t4x4_w8_s6_r512_u1_cap", float, 8, 8, 4, 4, 8, 6, 512, 1, false),
+    TSM_BULK_VARIANT("bulkf32_16x16_t8x8_w8_s6_r256_u1_cap", float, 16, 16, 8, 8, 8, 6, 256, 1, false),
+    TSM_BULK_VARIANT("bulkf32_32x32_t8x8_w8_s6_r128_u1_cap", float, 32, 32, 8, 8, 8, 6, 128, 1, false),
+    TSM_BULK_VARIANT("bulkf32_64x64_t8x8_w8_s6_r64_u1_cap", float, 64, 64, 8, 8, 8, 6, 64, 1, false),
+    TSM_DIRECT_VARIANT("directf32_2x1_t2x1_th256_cap", float, 2, 1, 2, 1, 256, false),
+    TSM_DIRECT_VARIANT("directf32_4x2_t4x2_th256_cap", float, 4, 2, 4, 2, 256, false),
+    TSM_DIRECT_VARIANT("directf32_8x4_t4x4_th256_cap", float, 8, 4, 4, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_16x8_t8x4_th256_cap", float, 16, 8, 8, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_32x16_t8x8_th256_cap", float, 32, 16, 8, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_64x32_t8x8_th256_cap", float, 64, 32, 8, 8, 256, false),
 };
 extern const int kGenPart3Count;
-const int kGenPart3Count = 17;
+const int kGenPart3Count = 30;
 
 }  // namespace tsm

@@ -91,7 +91,9 @@ tsm_status prepare_variant(DeviceState* st, int idx) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-bool applicable(const Variant* v, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
+bool applicable(const Variant* v, int dtype, int m, int k, const void* A, int64_t lda, const void* B,
+                int64_t ldb) {
+  if (v->dtype != dtype) return false;
   if (v->exact ? (m != v->wa || k != v->wb) : (m > v->wa || k > v->wb)) return false;
   if (v->kind == kKindBulk) {
     if (lda != m || ldb != k) return false;
@@ -115,7 +117,7 @@ int find_variant(const char* name) {
   return -1;
 }
 
-int default_variant(int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
+int default_variant(int dtype, int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
   const auto& vs = variants();
   // 1. The tuning table: the entry with the largest nmin <= n for (m, k).
   int best = -1;
@@ -127,7 +129,7 @@ int default_variant(int64_t n, int m, int k, const void* A, int64_t lda, const v
     if (std::sscanf(kTunedDefaults[i], "%d %d %lld %95s", &tm, &tk, &nmin, name) != 4) continue;
     if (tm != m || tk != k || nmin > n || nmin < best_nmin) continue;
     const int idx = find_variant(name);
-    if (idx >= 0 && applicable(vs[idx], m, k, A, lda, B, ldb)) {
+    if (idx >= 0 && applicable(vs[idx], dtype, m, k, A, lda, B, ldb)) {
       best = idx;
       best_nmin = nmin;
     }
@@ -136,8 +138,27 @@ int default_variant(int64_t n, int m, int k, const void* A, int64_t lda, const v
   // 2. Table order: the generator lists exact bulk variants first, then
   //    capacity bulk variants from the smallest capacity up, then direct ones.
   for (size_t i = 0; i < vs.size(); ++i)
-    if (applicable(vs[i], m, k, A, lda, B, ldb)) return static_cast<int>(i);
+    if (applicable(vs[i], dtype, m, k, A, lda, B, ldb)) return static_cast<int>(i);
   return -1;
+}
+
+// Rows the bulk kernels stream: every copy of rows * width elements must be a
+// multiple of 16 bytes, so up to three final rows may be left to the epilogue.
+int64_t bulk_rows(int64_t n, int m, int k, size_t esize) {
+  auto need = [esize](int w) {
+    const size_t bytes = static_cast<size_t>(w) * esize;
+    size_t g = 16;
+    size_t b = bytes;
+    while (b) {
+      const size_t t = g % b;
+      g = b;
+      b = t;
+    }
+    return static_cast<int64_t>(16 / g);
+  };
+  const int64_t ra = need(m), rb = need(k);
+  const int64_t r0 = ra > rb ? ra : rb;  // both are powers of two
+  return n - n % r0;
 }
 
 tsm_status check_args(int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb,
@@ -153,9 +174,10 @@ size_t workspace_bytes_for(int sms, int m, int k) {
   return kWsHeader + static_cast<size_t>(sms) * kMaxCtasPerSm * m * k * sizeof(double);
 }
 
-tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
-                        const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate, void* ws,
-                        size_t ws_bytes, int variant) {
+template <typename T>
+tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const T* A, int64_t lda, const T* B,
+                        int64_t ldb, T* C, int64_t ldc, int accumulate, void* ws, size_t ws_bytes, int variant) {
+  constexpr int dtype = DTypeOf<T>::value;
   tsm_status s = check_args(n, m, k, A, lda, B, ldb, C, ldc);
   if (s != TSM_SUCCESS) return s;
   int dev = 0;
@@ -167,15 +189,15 @@ tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const doub
   const auto& vs = variants();
   int idx = variant;
   if (idx < 0) {
-    idx = default_variant(n, m, k, A, lda, B, ldb);
+    idx = default_variant(dtype, n, m, k, A, lda, B, ldb);
     if (idx < 0) return TSM_ERROR_UNSUPPORTED;
-  } else if (idx >= static_cast<int>(vs.size()) || !applicable(vs[idx], m, k, A, lda, B, ldb)) {
+  } else if (idx >= static_cast<int>(vs.size()) || !applicable(vs[idx], dtype, m, k, A, lda, B, ldb)) {
     return TSM_ERROR_UNSUPPORTED;
   }
   if ((s = prepare_variant(st, idx)) != TSM_SUCCESS) return s;
   const Variant* v = vs[idx];
 
-  PlainArgs p{};
+  PlainArgs<T> p{};
   p.A = A;
   p.B = B;
   p.C = C;
@@ -194,9 +216,9 @@ tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const doub
   const int64_t max_grid = static_cast<int64_t>(st->sms) * st->occupancy[idx];
   int64_t grid = 1;
   if (v->kind == kKindBulk) {
-    // 16-byte bulk copies: an odd final row of an odd-width operand is left
-    // to the reduction epilogue.
-    p.rows_main = ((m % 2 == 0) && (k % 2 == 0)) ? n : (n & ~int64_t(1));
+    // 16-byte bulk copies: up to three final rows of an odd-width operand
+    // are left to the reduction epilogue.
+    p.rows_main = bulk_rows(n, m, k, sizeof(T));
     p.num_chunks = (p.rows_main + v->rows - 1) / v->rows;
     grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, max_grid));
   } else {
@@ -262,20 +284,36 @@ size_t tsm_gemm_tn_workspace_size(int64_t n, int m, int k) {
 tsm_status tsm_gemm_tn_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
                            const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate, void* workspace,
                            size_t workspace_bytes) {
-  return launch_plain(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate, workspace,
-                      workspace_bytes, -1);
+  return launch_plain<double>(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate,
+                              workspace, workspace_bytes, -1);
 }
 
 tsm_status tsm_gemm_tn_f64_variant(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
                                    const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
                                    void* workspace, size_t workspace_bytes, int variant) {
-  return launch_plain(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate, workspace,
-                      workspace_bytes, variant);
+  return launch_plain<double>(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate,
+                              workspace, workspace_bytes, variant);
 }
 
-int tsm_gemm_tn_default_variant(int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
+tsm_status tsm_gemm_tn_f32(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                           const float* B, int64_t ldb, float* C, int64_t ldc, int accumulate, void* workspace,
+                           size_t workspace_bytes) {
+  return launch_plain<float>(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate,
+                             workspace, workspace_bytes, -1);
+}
+
+tsm_status tsm_gemm_tn_f32_variant(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                                   const float* B, int64_t ldb, float* C, int64_t ldc, int accumulate,
+                                   void* workspace, size_t workspace_bytes, int variant) {
+  return launch_plain<float>(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate,
+                             workspace, workspace_bytes, variant);
+}
+
+int tsm_gemm_tn_default_variant(int dtype, int64_t n, int m, int k, const void* A, int64_t lda, const void* B,
+                                int64_t ldb) {
+  if (dtype != kF64 && dtype != kF32) return -1;
   if (check_args(n, m, k, A, lda, B, ldb, A ? A : B, k) != TSM_SUCCESS) return -1;
-  return default_variant(n, m, k, A, lda, B, ldb);
+  return default_variant(dtype, n, m, k, A, lda, B, ldb);
 }
 
 int tsm_variant_count(void) { return static_cast<int>(variants().size()); }
@@ -286,6 +324,7 @@ tsm_status tsm_variant_get_info(int index, tsm_variant_info* info) {
   std::memset(info, 0, sizeof(*info));
   std::strncpy(info->name, v->name, sizeof(info->name) - 1);
   info->kind = v->kind;
+  info->dtype = v->dtype;
   info->wa = v->wa;
   info->wb = v->wb;
   info->ta = v->ta;
@@ -401,12 +440,12 @@ extern "C" tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, in
   if ((s = static_scratch(dev, &scratch)) != TSM_SUCCESS) return s;
 
   // Same variant and grid as tsm_gemm_tn_f64 would use.
-  const int idx = default_variant(n, m, k, A, lda, B, ldb);
+  const int idx = default_variant(kF64, n, m, k, A, lda, B, ldb);
   if (idx < 0) return TSM_ERROR_UNSUPPORTED;
   if ((s = prepare_variant(st, idx)) != TSM_SUCCESS) return s;
   const Variant* v = variants()[idx];
 
-  PlainArgs p{};
+  PlainArgs<double> p{};
   p.A = A;
   p.B = B;
   p.C = C;
@@ -420,7 +459,7 @@ extern "C" tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, in
   const int64_t max_grid = static_cast<int64_t>(st->sms) * st->occupancy[idx];
   int64_t grid = 1;
   if (v->kind == kKindBulk) {
-    p.rows_main = ((m % 2 == 0) && (k % 2 == 0)) ? n : (n & ~int64_t(1));
+    p.rows_main = bulk_rows(n, m, k, sizeof(double));
     p.num_chunks = (p.rows_main + v->rows - 1) / v->rows;
     grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, max_grid));
   } else {

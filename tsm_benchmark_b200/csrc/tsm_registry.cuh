@@ -15,10 +15,23 @@
 namespace tsm {
 
 enum VariantKind : int { kKindBulk = 0, kKindDirect = 1 };
+enum DType : int { kF64 = 0, kF32 = 1 };
+
+template <typename T>
+struct DTypeOf;
+template <>
+struct DTypeOf<double> {
+  static constexpr int value = kF64;
+};
+template <>
+struct DTypeOf<float> {
+  static constexpr int value = kF32;
+};
 
 struct Variant {
   const char* name;
   int kind;     // VariantKind
+  int dtype;    // DType of A, B and C
   int wa, wb;   // widths (exact) or capacities
   int ta, tb;   // per-thread tile of C
   int exact;    // 1: only m == wa && k == wb; 0: any m <= wa, k <= wb
@@ -41,16 +54,17 @@ extern const int kVariantPartCount;
 
 }  // namespace tsm
 
-#define TSM_BULK_VARIANT(NAME, WA, WB, TA, TB, CW, ST, RS, U, EX)                                       \
-  ::tsm::Variant {                                                                                    \
-    NAME, ::tsm::kKindBulk, WA, WB, TA, TB, EX, ::tsm::BulkKernel<WA, WB, TA, TB, CW, ST, RS, U, EX>::THREADS, \
-        ST, RS, U, ::tsm::BulkKernel<WA, WB, TA, TB, CW, ST, RS, U, EX>::SMEM_BYTES,                   \
-        reinterpret_cast<const void*>(&::tsm::tsm_tn_bulk_kernel<WA, WB, TA, TB, CW, ST, RS, U, EX>)  \
+#define TSM_BULK_VARIANT(NAME, T, WA, WB, TA, TB, CW, ST, RS, U, EX)                                     \
+  ::tsm::Variant {                                                                                       \
+    NAME, ::tsm::kKindBulk, ::tsm::DTypeOf<T>::value, WA, WB, TA, TB, EX,                                \
+        ::tsm::BulkKernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX>::THREADS, ST, RS, U,                     \
+        ::tsm::BulkKernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX>::SMEM_BYTES,                             \
+        reinterpret_cast<const void*>(&::tsm::tsm_tn_bulk_kernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX>)  \
   }
 
-#define TSM_DIRECT_VARIANT(NAME, WA, WB, TA, TB, TH, EX)                                              \
-  ::tsm::Variant {                                                                                    \
-    NAME, ::tsm::kKindDirect, WA, WB, TA, TB, EX, TH, 0, 0, 1,                                        \
-        ::tsm::DirectKernel<WA, WB, TA, TB, TH, EX>::SMEM_BYTES,                                      \
-        reinterpret_cast<const void*>(&::tsm::tsm_tn_direct_kernel<WA, WB, TA, TB, TH, EX>)           \
+#define TSM_DIRECT_VARIANT(NAME, T, WA, WB, TA, TB, TH, EX)                                        \
+  ::tsm::Variant {                                                                                 \
+    NAME, ::tsm::kKindDirect, ::tsm::DTypeOf<T>::value, WA, WB, TA, TB, EX, TH, 0, 0, 1,           \
+        ::tsm::DirectKernel<T, WA, WB, TA, TB, TH, EX>::SMEM_BYTES,                                \
+        reinterpret_cast<const void*>(&::tsm::tsm_tn_direct_kernel<T, WA, WB, TA, TB, TH, EX>)     \
   }

@@ -1,0 +1,252 @@
+// tsm_tsmm.cu -- C ABI of the backward products (TSMM) and of the fused
+// backward of C = A^T B.  Kernels: csrc/tsm_tsmm.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "../../include/tsm.h"
+#include "tsm_tsmm.cuh"
+
+namespace tsm {
+namespace {
+
+constexpr int kCW = 8, kStages = 4;
+
+// Rows per chunk: ~32 KB stages, whole passes of the row groups.
+template <typename T, int C>
+constexpr int tsmm_rows() {
+  constexpr int wpr = C >= 32 ? C / 32 : 1;
+  constexpr int rw = C >= 32 ? 1 : 32 / C;
+  constexpr int rgn = (kCW / wpr) * rw;
+  constexpr int epc = 16 / int(sizeof(T));
+  constexpr int unit = rgn > epc ? rgn : epc;  // both are powers of two
+  constexpr int rows = 32768 / (C * int(sizeof(T)));
+  return rows / unit * unit;
+}
+
+struct TsmmEntry {
+  int dtype;  // 0 f64, 1 f32
+  int cap;
+  const void* bulk;
+  int bulk_threads;
+  size_t bulk_smem;
+  int rows;
+  const void* direct;
+};
+
+#define TSM_TSMM_ENTRY(T, DT, C)                                                                          \
+  TsmmEntry {                                                                                             \
+    DT, C, reinterpret_cast<const void*>(&tsm_tsmm_bulk_kernel<T, C, kCW, kStages, tsmm_rows<T, C>()>),   \
+        TsmmKernel<T, C, kCW, kStages, tsmm_rows<T, C>()>::THREADS,                                       \
+        TsmmKernel<T, C, kCW, kStages, tsmm_rows<T, C>()>::SMEM_BYTES, tsmm_rows<T, C>(),                 \
+        reinterpret_cast<const void*>(&tsm_tsmm_direct_kernel<T, C, 256>)                                 \
+  }
+
+const TsmmEntry kTsmm[] = {
+    TSM_TSMM_ENTRY(double, 0, 1),  TSM_TSMM_ENTRY(double, 0, 2),  TSM_TSMM_ENTRY(double, 0, 4),
+    TSM_TSMM_ENTRY(double, 0, 8),  TSM_TSMM_ENTRY(double, 0, 16), TSM_TSMM_ENTRY(double, 0, 32),
+    TSM_TSMM_ENTRY(double, 0, 64), TSM_TSMM_ENTRY(float, 1, 1),   TSM_TSMM_ENTRY(float, 1, 2),
+    TSM_TSMM_ENTRY(float, 1, 4),   TSM_TSMM_ENTRY(float, 1, 8),   TSM_TSMM_ENTRY(float, 1, 16),
+    TSM_TSMM_ENTRY(float, 1, 32),  TSM_TSMM_ENTRY(float, 1, 64),
+};
+constexpr int kTsmmCount = sizeof(kTsmm) / sizeof(kTsmm[0]);
+
+thread_local std::string g_tsmm_error;
+std::mutex g_tsmm_mu;
+int g_sms[64] = {};
+signed char g_ready[64][kTsmmCount] = {};
+
+tsm_status fail(cudaError_t e, const char* what) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  g_tsmm_error = buf;
+  return TSM_ERROR_CUDA;
+}
+
+int cap_of(int w) {
+  int c = 1;
+  while (c < w) c <<= 1;
+  return c;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int64_t tsmm_bulk_rows(int64_t n, int p, size_t esize) {
+  const size_t bytes = static_cast<size_t>(p) * esize;
+  size_t g = 16, b = bytes;
+  while (b) {
+    const size_t t = g % b;
+    g = b;
+    b = t;
+  }
+  const int64_t r0 = static_cast<int64_t>(16 / g);
+  return n - n % r0;
+}
+
+template <typename T>
+tsm_status launch_tsmm(cudaStream_t stream, TsmmProblem<T>* probs, int nprob, void* ws, size_t ws_bytes) {
+  constexpr int dtype = sizeof(T) == 8 ? 0 : 1;
+  if (ws == nullptr || ws_bytes < 256 || !aligned16(ws)) return TSM_ERROR_WORKSPACE;
+  int cap = 1;
+  bool bulk = true;
+  for (int i = 0; i < nprob; ++i) {
+    const TsmmProblem<T>& pr = probs[i];
+    if (pr.n < 0 || pr.p < 1 || pr.q < 1 || pr.p > 64 || pr.q > 64) return TSM_ERROR_INVALID_VALUE;
+    if (pr.ldx < pr.p || pr.ldy < pr.q || pr.W == nullptr) return TSM_ERROR_INVALID_VALUE;
+    if (pr.n > 0 && (pr.X == nullptr || pr.Y == nullptr)) return TSM_ERROR_INVALID_VALUE;
+    cap = std::max(cap, std::max(cap_of(pr.p), cap_of(pr.q)));
+    if (pr.ldx != pr.p || !aligned16(pr.X)) bulk = false;
+  }
+  int idx = -1;
+  for (int i = 0; i < kTsmmCount; ++i)
+    if (kTsmm[i].dtype == dtype && kTsmm[i].cap == cap) idx = i;
+  if (idx < 0) return TSM_ERROR_UNSUPPORTED;
+  const TsmmEntry& e = kTsmm[idx];
+
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) return fail(ce, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return TSM_ERROR_UNSUPPORTED;
+  {
+    std::lock_guard<std::mutex> lk(g_tsmm_mu);
+    if (g_sms[dev] == 0) {
+      ce = cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+      if (ce != cudaSuccess) return fail(ce, "cudaDeviceGetAttribute");
+    }
+    if (!g_ready[dev][idx]) {
+      ce = cudaFuncSetAttribute(e.bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(e.bulk_smem));
+      if (ce != cudaSuccess) return fail(ce, "cudaFuncSetAttribute");
+      g_ready[dev][idx] = 1;
+    }
+  }
+  const int sms = g_sms[dev];
+
+  TsmmArgs<T> a{};
+  a.nprob = nprob;
+  a.error = reinterpret_cast<unsigned*>(ws) + 1;
+  for (int i = 0; i < nprob; ++i) a.prob[i] = probs[i];
+  cudaError_t le;
+  if (bulk) {
+    int64_t total = 0;
+    for (int i = 0; i < nprob; ++i) {
+      TsmmProblem<T>& pr = a.prob[i];
+      pr.rows_main = tsmm_bulk_rows(pr.n, pr.p, sizeof(T));
+      pr.num_chunks = (pr.rows_main + e.rows - 1) / e.rows;
+      if (i == 0) a.split = pr.num_chunks;
+      total += pr.num_chunks;
+    }
+    if (nprob == 1) a.split = total;
+    a.total_chunks = total;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(total, sms));
+    void* args[] = {&a};
+    le = cudaLaunchKernel(e.bulk, dim3(static_cast<unsigned>(grid)), dim3(e.bulk_threads), args, e.bulk_smem,
+                          stream);
+  } else {
+    int64_t nmax = 0;
+    for (int i = 0; i < nprob; ++i) nmax = std::max(nmax, a.prob[i].n);
+    const int rgn = cap >= 32 ? (8 / (cap / 32)) : 8 * (32 / cap);
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nmax + rgn - 1) / rgn, int64_t(sms) * 8));
+    void* args[] = {&a};
+    le = cudaLaunchKernel(e.direct, dim3(static_cast<unsigned>(grid)), dim3(256), args, 0, stream);
+  }
+  if (le != cudaSuccess) return fail(le, "cudaLaunchKernel(tsmm)");
+  return TSM_SUCCESS;
+}
+
+template <typename T>
+tsm_status tsmm_entry(tsm_stream_t stream, int64_t n, int p, int q, const T* X, int64_t ldx, const T* W,
+                      int64_t w_row, int64_t w_col, T* Y, int64_t ldy, int beta, void* ws, size_t ws_bytes) {
+  TsmmProblem<T> pr{};
+  pr.X = X;
+  pr.ldx = ldx;
+  pr.W = W;
+  pr.w_row = w_row;
+  pr.w_col = w_col;
+  pr.Y = Y;
+  pr.ldy = ldy;
+  pr.n = n;
+  pr.p = p;
+  pr.q = q;
+  pr.beta = beta ? 1 : 0;
+  return launch_tsmm<T>(static_cast<cudaStream_t>(stream), &pr, 1, ws, ws_bytes);
+}
+
+template <typename T>
+tsm_status backward_entry(tsm_stream_t stream, int64_t n, int m, int k, const T* A, int64_t lda, const T* B,
+                          int64_t ldb, const T* dC, int64_t lddc, T* dA, int64_t ldda, T* dB, int64_t lddb, int beta,
+                          void* ws, size_t ws_bytes) {
+  if (m < 1 || k < 1 || m > 64 || k > 64 || lddc < k || dC == nullptr) return TSM_ERROR_INVALID_VALUE;
+  TsmmProblem<T> pr[2] = {};
+  int np = 0;
+  if (dA != nullptr) {  // dA (n x m) = B (n x k) * dC^T: W[a][b] = dC[b][a]
+    TsmmProblem<T>& x = pr[np++];
+    x.X = B;
+    x.ldx = ldb;
+    x.W = dC;
+    x.w_row = 1;
+    x.w_col = lddc;
+    x.Y = dA;
+    x.ldy = ldda;
+    x.n = n;
+    x.p = k;
+    x.q = m;
+    x.beta = beta ? 1 : 0;
+  }
+  if (dB != nullptr) {  // dB (n x k) = A (n x m) * dC
+    TsmmProblem<T>& x = pr[np++];
+    x.X = A;
+    x.ldx = lda;
+    x.W = dC;
+    x.w_row = lddc;
+    x.w_col = 1;
+    x.Y = dB;
+    x.ldy = lddb;
+    x.n = n;
+    x.p = m;
+    x.q = k;
+    x.beta = beta ? 1 : 0;
+  }
+  if (np == 0) return TSM_SUCCESS;
+  return launch_tsmm<T>(static_cast<cudaStream_t>(stream), pr, np, ws, ws_bytes);
+}
+
+}  // namespace
+}  // namespace tsm
+
+using namespace tsm;
+
+extern "C" {
+
+tsm_status tsm_tsmm_f64(tsm_stream_t stream, int64_t n, int p, int q, const double* X, int64_t ldx, const double* W,
+                        int64_t w_row, int64_t w_col, double* Y, int64_t ldy, int beta, void* workspace,
+                        size_t workspace_bytes) {
+  return tsmm_entry<double>(stream, n, p, q, X, ldx, W, w_row, w_col, Y, ldy, beta, workspace, workspace_bytes);
+}
+
+tsm_status tsm_tsmm_f32(tsm_stream_t stream, int64_t n, int p, int q, const float* X, int64_t ldx, const float* W,
+                        int64_t w_row, int64_t w_col, float* Y, int64_t ldy, int beta, void* workspace,
+                        size_t workspace_bytes) {
+  return tsmm_entry<float>(stream, n, p, q, X, ldx, W, w_row, w_col, Y, ldy, beta, workspace, workspace_bytes);
+}
+
+tsm_status tsm_gemm_tn_backward_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                                    const double* B, int64_t ldb, const double* dC, int64_t lddc, double* dA,
+                                    int64_t ldda, double* dB, int64_t lddb, int beta, void* workspace,
+                                    size_t workspace_bytes) {
+  return backward_entry<double>(stream, n, m, k, A, lda, B, ldb, dC, lddc, dA, ldda, dB, lddb, beta, workspace,
+                                workspace_bytes);
+}
+
+tsm_status tsm_gemm_tn_backward_f32(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                                    const float* B, int64_t ldb, const float* dC, int64_t lddc, float* dA,
+                                    int64_t ldda, float* dB, int64_t lddb, int beta, void* workspace,
+                                    size_t workspace_bytes) {
+  return backward_entry<float>(stream, n, m, k, A, lda, B, ldb, dC, lddc, dA, ldda, dB, lddb, beta, workspace,
+                               workspace_bytes);
+}
+
+}  // extern "C"
