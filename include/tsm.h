@@ -94,6 +94,19 @@ tsm_status tsm_gemm_tn_f32_variant(tsm_stream_t stream, int64_t n, int m, int k,
                                    const float* B, int64_t ldb, float* C, int64_t ldc, int accumulate,
                                    void* workspace, size_t workspace_bytes, int variant);
 
+/* The precision form: C (FP64) = A^T B (accumulate = 0) or C += A^T B for
+ * FP32-stored A, B on the tcgen05 tensor cores, 1 <= m, k <= 32, A and B
+ * contiguous (lda = m, ldb = k) and 16-byte aligned.  Each FP32 value is
+ * split into TF32 hi = rna(x) and lo = rna(x - hi) (|x - hi - lo| <=
+ * 2^-23 |x|); one tcgen05.mma per 8 rows forms hi.hi + hi.lo + lo.hi + lo.lo
+ * with FP32 accumulation, drained to FP64 every 64 rows; every later sum is
+ * FP64 and fixed-order (deterministic).  Reads half the bytes of the FP64
+ * path on the same values.  No counterpart in the reference (its kernels are
+ * FP64 only).  Workspace: as tsm_gemm_tn_workspace_size(n, m, k). */
+tsm_status tsm_gemm_tn_f32_split(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                                 const float* B, int64_t ldb, double* C, int64_t ldc, int accumulate, void* workspace,
+                                 size_t workspace_bytes);
+
 /* Element types of the plain entry points. */
 #define TSM_F64 0
 #define TSM_F32 1

@@ -7,7 +7,7 @@ the autotuner.
 """
 from ._capi import TsmError, TsmLibraryError, variants  # noqa: F401
 from .api import (default_variant, fill_uniform, tsmm, tsmttsm, tsmttsm_backward,  # noqa: F401
-                  workspace_status)
+                  tsmttsm_split, workspace_status)
 from .autograd import TSMTTSMFunction, gram_tn  # noqa: F401
 from .batched import BatchedTSMTTSM  # noqa: F401
 

@@ -79,6 +79,8 @@ SIGNATURES = {
                                 c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_f32_variant": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int, c_void_p, c_size_t, c_int]),
+    "tsm_gemm_tn_f32_split": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                      c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_default_variant": (c_int, [c_int, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64]),
     "tsm_variant_count": (c_int, []),
     "tsm_variant_get_info": (c_int, [c_int, ctypes.POINTER(VariantInfo)]),

@@ -200,3 +200,31 @@ def tsmttsm_backward(A: torch.Tensor, B: torch.Tensor, dC: torch.Tensor, *, need
                                           ws.numel())
         _capi.check(st, _BWD[A.dtype])
     return dA, dB
+
+
+def tsmttsm_split(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, accumulate: bool = False,
+                  stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """C (float64) = A^T B for float32 A, B (m, k <= 32) on the tensor cores:
+    TF32 hi/lo split, FP32 accumulation per 64 rows, FP64 sums
+    (``tsm_gemm_tn_f32_split``)."""
+    _check_operand(A, "A", torch.float32)
+    _check_operand(B, "B", torch.float32)
+    n, m = A.shape
+    k = B.shape[1]
+    if B.shape[0] != n:
+        raise ValueError("A and B must have the same number of rows")
+    if C is None:
+        if accumulate:
+            raise ValueError("accumulate=True needs an existing C")
+        C = torch.empty((m, k), dtype=torch.float64, device=A.device)
+    else:
+        _check_operand(C, "C", torch.float64)
+    lib = _capi.load()
+    with torch.cuda.device(A.device):
+        sh = _stream_handle(A.device, stream)
+        need = lib.tsm_gemm_tn_workspace_size(n, m, k)
+        ws = workspace(A.device, need, sh)
+        st = lib.tsm_gemm_tn_f32_split(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
+                                       _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel())
+        _capi.check(st, "tsm_gemm_tn_f32_split")
+    return C

@@ -1,0 +1,98 @@
+// tsm_split.cu -- C ABI of the precision form (FP32 storage, TF32 hi/lo
+// split on tcgen05 tensor cores, FP64 reductions).  Kernel: tsm_split.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "../../include/tsm.h"
+#include "tsm_split.cuh"
+
+namespace tsm {
+namespace {
+
+std::mutex g_split_mu;
+int g_split_sms[64] = {};
+bool g_split_attr[64] = {};
+thread_local std::string g_split_error;
+
+tsm_status split_fail(cudaError_t e, const char* what) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  g_split_error = buf;
+  return TSM_ERROR_CUDA;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int64_t rows_for_bulk(int64_t n, int m, int k) {
+  auto need = [](int w) {
+    const int bytes = 4 * w;
+    int g = 16, b = bytes;
+    while (b) {
+      const int t = g % b;
+      g = b;
+      b = t;
+    }
+    return static_cast<int64_t>(16 / g);
+  };
+  const int64_t r0 = std::max(need(m), need(k));
+  return n - n % r0;
+}
+
+}  // namespace
+}  // namespace tsm
+
+using namespace tsm;
+
+extern "C" tsm_status tsm_gemm_tn_f32_split(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                                            const float* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
+                                            void* workspace, size_t workspace_bytes) {
+  if (n < 0 || m < 1 || k < 1 || m > 32 || k > 32 || ldc < k || C == nullptr) return TSM_ERROR_INVALID_VALUE;
+  if (n > 0 && (A == nullptr || B == nullptr)) return TSM_ERROR_INVALID_VALUE;
+  if (lda != m || ldb != k || !aligned16(A) || !aligned16(B)) return TSM_ERROR_UNSUPPORTED;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return split_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return TSM_ERROR_UNSUPPORTED;
+  {
+    std::lock_guard<std::mutex> lk(g_split_mu);
+    if (g_split_sms[dev] == 0) {
+      e = cudaDeviceGetAttribute(&g_split_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return split_fail(e, "cudaDeviceGetAttribute");
+    }
+    if (!g_split_attr[dev]) {
+      e = cudaFuncSetAttribute(reinterpret_cast<const void*>(&tsm_tn_split_tf32_kernel),
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(split::kSmemBytes));
+      if (e != cudaSuccess) return split_fail(e, "cudaFuncSetAttribute(split)");
+      g_split_attr[dev] = true;
+    }
+  }
+  const int sms = g_split_sms[dev];
+  const size_t need = 256 + static_cast<size_t>(sms) * 4 * m * k * sizeof(double);
+  if (workspace == nullptr || workspace_bytes < need || !aligned16(workspace)) return TSM_ERROR_WORKSPACE;
+  SplitArgs p{};
+  p.A = A;
+  p.B = B;
+  p.C = C;
+  p.n = n;
+  p.m = m;
+  p.k = k;
+  p.ldc = ldc;
+  p.accumulate = accumulate ? 1 : 0;
+  p.rows_main = rows_for_bulk(n, m, k);
+  p.num_chunks = (p.rows_main + split::kRows - 1) / split::kRows;
+  unsigned char* base = static_cast<unsigned char*>(workspace);
+  p.counter = reinterpret_cast<unsigned*>(base);
+  p.error = reinterpret_cast<unsigned*>(base) + 1;
+  p.partials = reinterpret_cast<double*>(base + 256);
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, sms));
+  void* args[] = {&p};
+  e = cudaLaunchKernel(reinterpret_cast<const void*>(&tsm_tn_split_tf32_kernel), dim3(static_cast<unsigned>(grid)),
+                       dim3(split::kThreads), args, split::kSmemBytes, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return split_fail(e, "cudaLaunchKernel(split)");
+  return TSM_SUCCESS;
+}
