@@ -196,6 +196,112 @@ def workload_config(n_gpus: int) -> dict:
             "l2": "inputs (8 GiB) larger than L2, no flush", "parallelism": f"rows sharded, {n_gpus} GPU(s)"}
 
 
+# -------------------------------------------------------------- the forms
+def _time(fn, reps: int, warmup: int = 3) -> float:
+    """Milliseconds per call, CUDA events on the current stream."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def forms(dev) -> dict:
+    """The three forms beside the plain FP64 path, each against FP64 on the
+    same GPU: split precision (n = 2^25, m = k = 32, FP32 storage, column
+    scaled normal data), batched (512 problems, one launch under a CUDA graph
+    vs one plain launch per problem) and differentiation (n = 2^22,
+    m = k = 16: fused backward vs forward time, FP64 and FP32)."""
+    import numpy as np
+    import torch
+
+    import tsm_benchmark_b200 as tsm
+    out = {}
+
+    # --- precision: TF32 hi/lo split on tcgen05 vs plain FP64 on FP64 copies
+    n, w = 1 << 25, 32
+    g = torch.Generator(device=dev).manual_seed(3)
+    sa = 10.0 ** (torch.rand(w, device=dev, generator=g) * 6 - 3)
+    sb = 10.0 ** (torch.rand(w, device=dev, generator=g) * 6 - 3)
+    A32 = (torch.randn((n, w), device=dev, generator=g) * sa).float()
+    B32 = (torch.randn((n, w), device=dev, generator=g) * sb).float()
+    A64, B64 = A32.double(), B32.double()
+    C_split = torch.empty((w, w), dtype=torch.float64, device=dev)
+    C_ref = torch.empty((w, w), dtype=torch.float64, device=dev)
+    ms_split = _time(lambda: tsm.tsmttsm_split(A32, B32, C_split), 20)
+    ms_f64 = _time(lambda: tsm.tsmttsm(A64, B64, C_ref), 20)
+    scale = tsm.tsmttsm(A64.abs(), B64.abs())
+    nw = float(torch.linalg.norm(C_split - C_ref) / torch.linalg.norm(C_ref))
+    pe = float(((C_split - C_ref).abs() / scale).max())
+    out["split_tf32"] = {"n": n, "m": w, "k": w, "ms": round(ms_split, 4), "fp64_ms": round(ms_f64, 4),
+                         "speedup_vs_fp64": round(ms_f64 / ms_split, 3),
+                         "GB/s": round(4 * n * 2 * w / (ms_split * 1e-3) / 1e9, 1),
+                         "err_normwise_rel": nw, "err_entry_max_rel": pe, "stated_err": 1e-6,
+                         "meets_stated_err": bool(nw <= 1e-6 and pe <= 1e-6)}
+    del A32, B32, A64, B64, scale
+    torch.cuda.empty_cache()
+
+    # --- batching: one persistent launch (graph replay) vs one launch per problem
+    rng = np.random.default_rng(5)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(1e6), size=512)).astype(np.int64)
+    ms_ = rng.choice((4, 8, 16, 32), size=512)
+    ks_ = rng.choice((4, 8, 16, 32), size=512)
+    As, Bs = [], []
+    for i, (nn, mm, kk) in enumerate(zip(ns, ms_, ks_)):
+        a = torch.empty((int(nn), int(mm)), dtype=torch.float64, device=dev)
+        b = torch.empty((int(nn), int(kk)), dtype=torch.float64, device=dev)
+        tsm.fill_uniform(a, 1000 + i, 0)
+        tsm.fill_uniform(b, 1000 + i, 1)
+        As.append(a)
+        Bs.append(b)
+    bt = tsm.BatchedTSMTTSM(As, Bs)
+    graph = bt.capture_graph()
+    ms_batched = _time(graph.replay, 20)
+    Cp = [torch.empty((a.shape[1], b.shape[1]), dtype=torch.float64, device=dev) for a, b in zip(As, Bs)]
+    lib = __import__("tsm_benchmark_b200._capi", fromlist=["load"]).load()
+    sh = int(torch.cuda.current_stream(dev).cuda_stream)
+    wsb = torch.zeros(lib.tsm_gemm_tn_workspace_size(1, 32, 32), dtype=torch.uint8, device=dev)
+
+    def plain_all():
+        for a, b, c in zip(As, Bs, Cp):
+            lib.tsm_gemm_tn_f64(sh, a.shape[0], a.shape[1], b.shape[1], a.data_ptr(), a.shape[1], b.data_ptr(),
+                                b.shape[1], c.data_ptr(), b.shape[1], 0, wsb.data_ptr(), wsb.numel())
+    ms_plain = _time(plain_all, 5, warmup=1)
+    err = max(float(torch.linalg.norm(c - p) / max(float(torch.linalg.norm(p)), 1e-300)) for c, p in zip(bt.Cs, Cp))
+    total_bytes = int(sum(8 * a.shape[0] * (a.shape[1] + b.shape[1]) for a, b in zip(As, Bs)))
+    out["batched"] = {"problems": 512, "bytes": total_bytes, "segments": bt.segments, "ms": round(ms_batched, 4),
+                      "plain_launches_ms": round(ms_plain, 4), "speedup_vs_fp64_plain": round(ms_plain / ms_batched, 3),
+                      "GB/s": round(total_bytes / (ms_batched * 1e-3) / 1e9, 1),
+                      "err_vs_plain_max_rel": err, "launches": 1, "cuda_graph": True}
+    del As, Bs, bt, graph, Cp
+    torch.cuda.empty_cache()
+
+    # --- differentiation: fused backward vs forward
+    n, w = 1 << 22, 16
+    for dt, name in ((torch.float64, "autograd_f64"), (torch.float32, "autograd_f32")):
+        A = (torch.rand((n, w), device=dev, generator=g, dtype=torch.float64) * 2 - 1).to(dt)
+        B = (torch.rand((n, w), device=dev, generator=g, dtype=torch.float64) * 2 - 1).to(dt)
+        Wl = torch.randn((w, w), device=dev, generator=g, dtype=torch.float64).to(dt)
+        C = torch.empty((w, w), dtype=dt, device=dev)
+        ms_fwd = _time(lambda: tsm.tsmttsm(A, B, C), 50)
+        ms_bwd = _time(lambda: tsm.tsmttsm_backward(A, B, Wl), 50)
+        esz = A.element_size()
+        out[name] = {"n": n, "m": w, "k": w, "fwd_ms": round(ms_fwd, 4), "bwd_ms": round(ms_bwd, 4),
+                     "bwd_over_fwd": round(ms_bwd / ms_fwd, 3),
+                     "fwd_GB/s": round(esz * n * 2 * w / (ms_fwd * 1e-3) / 1e9, 1),
+                     "bwd_GB/s": round(2 * esz * n * 2 * w / (ms_bwd * 1e-3) / 1e9, 1)}
+        del A, B
+        torch.cuda.empty_cache()
+    return out
+
+
 # ------------------------------------------------------------------ our arm
 def main() -> int:
     ap = argparse.ArgumentParser()
@@ -207,6 +313,7 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--ref-rows", type=int, default=1 << 23)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     args = ap.parse_args()
@@ -377,6 +484,13 @@ def main() -> int:
                "h2d_bytes_per_step": Ah.numel() * 8 + Bh.numel() * 8, "d2h_bytes_per_step": Ch.numel() * 8}
         del Ah, Bh
 
+    # ---------------- the precision, batching and differentiation forms
+    forms_out = None
+    if world == 1 and not args.no_forms:
+        del bufA, bufB, A, B
+        torch.cuda.empty_cache()
+        forms_out = forms(dev)
+
     # ---------------- CPU baseline (rank 0, N = 1)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -389,7 +503,7 @@ def main() -> int:
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(world),
                 "frac_hbm": value / world / peaks["hbm_gbs"], "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks, "by_width": by_width,
-                "checksum_ok": checksum_ok, "device_error_bits": dev_err}
+                "checksum_ok": checksum_ok, "device_error_bits": dev_err, "forms": forms_out}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

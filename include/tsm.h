@@ -99,7 +99,7 @@ tsm_status tsm_gemm_tn_f32_variant(tsm_stream_t stream, int64_t n, int m, int k,
  * contiguous (lda = m, ldb = k) and 16-byte aligned.  Each FP32 value is
  * split into TF32 hi = rna(x) and lo = rna(x - hi) (|x - hi - lo| <=
  * 2^-23 |x|); one tcgen05.mma per 8 rows forms hi.hi + hi.lo + lo.hi + lo.lo
- * with FP32 accumulation, drained to FP64 every 64 rows; every later sum is
+ * with FP32 accumulation, drained to FP64 every 128 rows; every later sum is
  * FP64 and fixed-order (deterministic).  Reads half the bytes of the FP64
  * path on the same values.  No counterpart in the reference (its kernels are
  * FP64 only).  Workspace: as tsm_gemm_tn_workspace_size(n, m, k). */

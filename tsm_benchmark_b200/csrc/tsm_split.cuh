@@ -7,10 +7,10 @@
 //     D = [A_hi ; A_lo]^T-stacked  x  [B_hi | B_lo]
 // so the four 32 x 32 quadrants of D are hi.hi, hi.lo, lo.hi and lo.lo; their
 // sum is C's contribution from those rows, with exact products and FP32
-// accumulation inside the tensor core.  Every 64 rows the FP32 accumulator is
-// drained from tensor memory into FP64 registers, which bounds the FP32
-// rounding to 64-row partial sums; all later sums (across drains, warps and
-// CTAs) are FP64, in a fixed order (deterministic).
+// accumulation inside the tensor core.  Every 128 rows (kFlush chunks) the
+// FP32 accumulator is drained from tensor memory into FP64 registers, which
+// bounds the FP32 rounding to 128-row partial sums; all later sums (across
+// drains, warps and CTAs) are FP64, in a fixed order (deterministic).
 //
 // Warp roles in one persistent CTA per SM (14 warps):
 //   warp 0      TMA producer: raw FP32 row chunks -> raw ring (1-D bulk copies)
@@ -54,6 +54,7 @@ struct SplitArgs {
 namespace split {
 
 constexpr int kRows = 64;         // rows per chunk (8 MMAs of K = 8)
+constexpr int kFlush = 2;         // chunks accumulated in one TMEM buffer (128 rows) before a drain
 constexpr int kRawStages = 4;
 constexpr int kOpStages = 2;
 constexpr int kConvWarps = 8;
@@ -172,11 +173,15 @@ __global__ void __launch_bounds__(split::kThreads, 1) tsm_tn_split_tf32_kernel(c
     const uint32_t op_base = dev::smem_u32(op_ring);
     for (int64_t it = 0; it < nchunks_mine; ++it) {
       const int o = static_cast<int>(it % kOpStages);
-      const int b = static_cast<int>(it & 1);
+      const int64_t grp = it / kFlush;  // accumulator group: kFlush chunks into one TMEM buffer
+      const int b = static_cast<int>(grp & 1);
+      const bool first = (it % kFlush) == 0;
+      const bool last = (it % kFlush) == kFlush - 1 || it == nchunks_mine - 1;
       bool ok = true;
       if (lane == 0) {
         ok = dev::mbar_wait(&op_full[o], static_cast<uint32_t>((it / kOpStages) & 1), abort);
-        if (ok && it >= 2) ok = dev::mbar_wait(&d_empty[b], static_cast<uint32_t>(((it >> 1) - 1) & 1), abort);
+        if (ok && first && grp >= 2)
+          ok = dev::mbar_wait(&d_empty[b], static_cast<uint32_t>(((grp >> 1) - 1) & 1), abort);
         if (ok) {
           dev::tc_fence_after();
           const uint32_t a_base = op_base + o * kOpStageBytes;
@@ -185,10 +190,10 @@ __global__ void __launch_bounds__(split::kThreads, 1) tsm_tn_split_tf32_kernel(c
           for (int g = 0; g < kRows / 8; ++g) {
             const uint64_t ad = dev::umma_smem_desc(a_base + g * 1024, kOpHalfBytes, kSbo, kLayout);
             const uint64_t bd = dev::umma_smem_desc(b_base + g * 1024, kOpHalfBytes, kSbo, kLayout);
-            dev::umma_tf32(tmem + b * 64, ad, bd, kIdesc, g > 0 ? 1u : 0u);
+            dev::umma_tf32(tmem + b * 64, ad, bd, kIdesc, (first && g == 0) ? 0u : 1u);
           }
-          dev::umma_commit(&op_empty[o]);  // operands may be overwritten once these MMAs are done
-          dev::umma_commit(&d_full[b]);    // accumulator b is complete
+          dev::umma_commit(&op_empty[o]);      // operands may be overwritten once these MMAs are done
+          if (last) dev::umma_commit(&d_full[b]);  // accumulator b holds its group's rows
         } else {
           *abort = 1;
           atomicOr(p.error, dev::kErrTimeout);
@@ -262,23 +267,27 @@ __global__ void __launch_bounds__(split::kThreads, 1) tsm_tn_split_tf32_kernel(c
     // ---------------- epilogue: TMEM -> FP64 sums (lanes 0-15 of each warp)
     const int q = warp & 3;
     const uint32_t lane_base = static_cast<uint32_t>(32 * q) << 16;
-    for (int64_t it = 0; it < nchunks_mine; ++it) {
-      const int b = static_cast<int>(it & 1);
-      if (!dev::mbar_wait(&d_full[b], static_cast<uint32_t>((it >> 1) & 1), abort)) {
+    const int64_t ngroups = (nchunks_mine + kFlush - 1) / kFlush;
+    for (int64_t grp = 0; grp < ngroups; ++grp) {
+      const int b = static_cast<int>(grp & 1);
+      if (!dev::mbar_wait(&d_full[b], static_cast<uint32_t>((grp >> 1) & 1), abort)) {
         *abort = 1;
         atomicOr(p.error, dev::kErrTimeout);
         break;
       }
       dev::tc_fence_after();
-      uint32_t v[32];
-      dev::tmem_ld32(tmem + lane_base + b * 64, v);  // columns 0..31: x B_hi
-      dev::tmem_ld_wait();
+      // Columns 0..31 hold x B_hi, 32..63 x B_lo (~2^-11 of the former): one
+      // FP32 addition, then one conversion to FP64.
 #pragma unroll
-      for (int j = 0; j < 32; ++j) acc[j] += static_cast<double>(__uint_as_float(v[j]));
-      dev::tmem_ld32(tmem + lane_base + b * 64 + 32, v);  // columns 32..63: x B_lo
-      dev::tmem_ld_wait();
+      for (int h = 0; h < 2; ++h) {
+        uint32_t v[16], u[16];
+        dev::tmem_ld16(tmem + lane_base + b * 64 + 16 * h, v);
+        dev::tmem_ld16(tmem + lane_base + b * 64 + 32 + 16 * h, u);
+        dev::tmem_ld_wait();
 #pragma unroll
-      for (int j = 0; j < 32; ++j) acc[j] += static_cast<double>(__uint_as_float(v[j]));
+        for (int j = 0; j < 16; ++j)
+          acc[16 * h + j] += static_cast<double>(__uint_as_float(v[j]) + __uint_as_float(u[j]));
+      }
       dev::tc_fence_before();
       __syncwarp();
       if (lane == 0) dev::mbar_arrive(&d_empty[b]);
@@ -295,8 +304,9 @@ __global__ void __launch_bounds__(split::kThreads, 1) tsm_tn_split_tf32_kernel(c
         if (!dev::mbar_wait(&raw_full[it % kRawStages], static_cast<uint32_t>((it / kRawStages) & 1), &no_abort))
           break;
     } else if (warp == 1) {
-      for (int64_t it = nchunks_mine > 2 ? nchunks_mine - 2 : 0; it < nchunks_mine; ++it)
-        if (!dev::mbar_wait(&d_full[it & 1], static_cast<uint32_t>((it >> 1) & 1), &no_abort)) break;
+      const int64_t ngroups = (nchunks_mine + kFlush - 1) / kFlush;
+      for (int64_t grp = ngroups > 2 ? ngroups - 2 : 0; grp < ngroups; ++grp)
+        if (!dev::mbar_wait(&d_full[grp & 1], static_cast<uint32_t>((grp >> 1) & 1), &no_abort)) break;
     }
   }
   dev::tc_fence_before();

@@ -10,41 +10,22 @@
 
 #include "../../include/tsm.h"
 #include "tsm_tsmm.cuh"
+#include "tsm_tsmm_dmma.cuh"
 
 namespace tsm {
 namespace {
 
 constexpr int kCW = 8, kStages = 4;
 
-// Rows per chunk: ~32 KB stages, whole passes of the row groups.
-template <typename T, int C>
-constexpr int tsmm_rows() {
-  constexpr int wpr = C >= 32 ? C / 32 : 1;
-  constexpr int rw = C >= 32 ? 1 : 32 / C;
-  constexpr int rgn = (kCW / wpr) * rw;
-  constexpr int epc = 16 / int(sizeof(T));
-  constexpr int unit = rgn > epc ? rgn : epc;  // both are powers of two
-  constexpr int rows = 32768 / (C * int(sizeof(T)));
-  return rows / unit * unit;
-}
-
+// SIMT kernels with direct loads: X with any row stride or alignment.
 struct TsmmEntry {
   int dtype;  // 0 f64, 1 f32
   int cap;
-  const void* bulk;
-  int bulk_threads;
-  size_t bulk_smem;
-  int rows;
   const void* direct;
 };
 
-#define TSM_TSMM_ENTRY(T, DT, C)                                                                          \
-  TsmmEntry {                                                                                             \
-    DT, C, reinterpret_cast<const void*>(&tsm_tsmm_bulk_kernel<T, C, kCW, kStages, tsmm_rows<T, C>()>),   \
-        TsmmKernel<T, C, kCW, kStages, tsmm_rows<T, C>()>::THREADS,                                       \
-        TsmmKernel<T, C, kCW, kStages, tsmm_rows<T, C>()>::SMEM_BYTES, tsmm_rows<T, C>(),                 \
-        reinterpret_cast<const void*>(&tsm_tsmm_direct_kernel<T, C, 256>)                                 \
-  }
+#define TSM_TSMM_ENTRY(T, DT, C) \
+  TsmmEntry { DT, C, reinterpret_cast<const void*>(&tsm_tsmm_direct_kernel<T, C, 256>) }
 
 const TsmmEntry kTsmm[] = {
     TSM_TSMM_ENTRY(double, 0, 1),  TSM_TSMM_ENTRY(double, 0, 2),  TSM_TSMM_ENTRY(double, 0, 4),
@@ -55,10 +36,44 @@ const TsmmEntry kTsmm[] = {
 };
 constexpr int kTsmmCount = sizeof(kTsmm) / sizeof(kTsmm[0]);
 
+// FP64 tensor-core (DMMA) kernels for dense, aligned X, FP64 or FP32
+// storage: capacities P, Q in {4, 8, 16, 32, 64}, ~32 KB stages.
+struct DmmaEntry {
+  int dtype;  // 0 f64, 1 f32
+  int P, Q;
+  const void* fn;
+  int threads;
+  size_t smem;
+  int rows;
+};
+
+template <typename T, int P>
+constexpr int dmma_rows() {
+  return 32768 / (P * int(sizeof(T)));
+}
+
+#define TSM_DMMA_ENTRY(T, DT, P, Q)                                                                            \
+  DmmaEntry {                                                                                                  \
+    DT, P, Q, reinterpret_cast<const void*>(&tsm_tsmm_dmma_kernel<T, P, Q, kCW, kStages, dmma_rows<T, P>()>),   \
+        TsmmDmmaKernel<T, P, Q, kCW, kStages, dmma_rows<T, P>()>::THREADS,                                      \
+        TsmmDmmaKernel<T, P, Q, kCW, kStages, dmma_rows<T, P>()>::SMEM_BYTES, dmma_rows<T, P>()                 \
+  }
+#define TSM_DMMA_ROW(T, DT, P)                                                                              \
+  TSM_DMMA_ENTRY(T, DT, P, 4), TSM_DMMA_ENTRY(T, DT, P, 8), TSM_DMMA_ENTRY(T, DT, P, 16),                   \
+      TSM_DMMA_ENTRY(T, DT, P, 32), TSM_DMMA_ENTRY(T, DT, P, 64)
+
+const DmmaEntry kDmma[] = {
+    TSM_DMMA_ROW(double, 0, 4),  TSM_DMMA_ROW(double, 0, 8), TSM_DMMA_ROW(double, 0, 16),
+    TSM_DMMA_ROW(double, 0, 32), TSM_DMMA_ROW(double, 0, 64), TSM_DMMA_ROW(float, 1, 4),
+    TSM_DMMA_ROW(float, 1, 8),   TSM_DMMA_ROW(float, 1, 16),  TSM_DMMA_ROW(float, 1, 32),
+    TSM_DMMA_ROW(float, 1, 64),
+};
+constexpr int kDmmaCount = sizeof(kDmma) / sizeof(kDmma[0]);
+
 thread_local std::string g_tsmm_error;
 std::mutex g_tsmm_mu;
 int g_sms[64] = {};
-signed char g_ready[64][kTsmmCount] = {};
+signed char g_dmma_ready[64][kDmmaCount] = {};
 
 tsm_status fail(cudaError_t e, const char* what) {
   char buf[256];
@@ -87,6 +102,69 @@ int64_t tsmm_bulk_rows(int64_t n, int p, size_t esize) {
   return n - n % r0;
 }
 
+// Splits the problems' streamed rows into chunks of `rows` rows.
+template <typename T>
+void set_chunks(TsmmArgs<T>& a, int rows) {
+  int64_t total = 0;
+  for (int i = 0; i < a.nprob; ++i) {
+    TsmmProblem<T>& pr = a.prob[i];
+    pr.rows_main = tsmm_bulk_rows(pr.n, pr.p, sizeof(T));
+    pr.num_chunks = (pr.rows_main + rows - 1) / rows;
+    if (i == 0) a.split = pr.num_chunks;
+    total += pr.num_chunks;
+  }
+  if (a.nprob == 1) a.split = total;
+  a.total_chunks = total;
+}
+
+int dmma_index(int dtype, int p, int q) {
+  const int P = std::max(4, cap_of(p)), Q = std::max(4, cap_of(q));
+  for (int i = 0; i < kDmmaCount; ++i)
+    if (kDmma[i].dtype == dtype && kDmma[i].P == P && kDmma[i].Q == Q) return i;
+  return -1;
+}
+
+// Bulk path on the FP64 tensor cores: one launch when both problems share
+// capacities (the fused backward of square or same-capacity shapes), else
+// one launch per problem.
+template <typename T>
+tsm_status launch_dmma(cudaStream_t stream, int dev, int sms, const TsmmProblem<T>* probs, int nprob,
+                       unsigned* error) {
+  constexpr int dtype = sizeof(T) == 8 ? 0 : 1;
+  int idx[2] = {dmma_index(dtype, probs[0].p, probs[0].q),
+                nprob > 1 ? dmma_index(dtype, probs[1].p, probs[1].q) : -1};
+  const bool together = nprob == 1 || idx[0] == idx[1];
+  for (int l = 0; l < (together ? 1 : nprob); ++l) {
+    const DmmaEntry& e = kDmma[idx[l]];
+    {
+      std::lock_guard<std::mutex> lk(g_tsmm_mu);
+      if (!g_dmma_ready[dev][idx[l]]) {
+        const cudaError_t ce =
+            cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(e.smem));
+        if (ce != cudaSuccess) return fail(ce, "cudaFuncSetAttribute(dmma)");
+        g_dmma_ready[dev][idx[l]] = 1;
+      }
+    }
+    TsmmArgs<T> a{};
+    a.error = error;
+    if (together) {
+      a.nprob = nprob;
+      for (int i = 0; i < nprob; ++i) a.prob[i] = probs[i];
+    } else {
+      a.nprob = 1;
+      a.prob[0] = probs[l];
+    }
+    set_chunks(a, e.rows);
+    if (a.total_chunks == 0 && a.prob[0].n == 0 && (a.nprob < 2 || a.prob[1].n == 0)) continue;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(a.total_chunks, sms));
+    void* args[] = {&a};
+    const cudaError_t le =
+        cudaLaunchKernel(e.fn, dim3(static_cast<unsigned>(grid)), dim3(e.threads), args, e.smem, stream);
+    if (le != cudaSuccess) return fail(le, "cudaLaunchKernel(tsmm dmma)");
+  }
+  return TSM_SUCCESS;
+}
+
 template <typename T>
 tsm_status launch_tsmm(cudaStream_t stream, TsmmProblem<T>* probs, int nprob, void* ws, size_t ws_bytes) {
   constexpr int dtype = sizeof(T) == 8 ? 0 : 1;
@@ -101,12 +179,6 @@ tsm_status launch_tsmm(cudaStream_t stream, TsmmProblem<T>* probs, int nprob, vo
     cap = std::max(cap, std::max(cap_of(pr.p), cap_of(pr.q)));
     if (pr.ldx != pr.p || !aligned16(pr.X)) bulk = false;
   }
-  int idx = -1;
-  for (int i = 0; i < kTsmmCount; ++i)
-    if (kTsmm[i].dtype == dtype && kTsmm[i].cap == cap) idx = i;
-  if (idx < 0) return TSM_ERROR_UNSUPPORTED;
-  const TsmmEntry& e = kTsmm[idx];
-
   int dev = 0;
   cudaError_t ce = cudaGetDevice(&dev);
   if (ce != cudaSuccess) return fail(ce, "cudaGetDevice");
@@ -117,42 +189,24 @@ tsm_status launch_tsmm(cudaStream_t stream, TsmmProblem<T>* probs, int nprob, vo
       ce = cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev);
       if (ce != cudaSuccess) return fail(ce, "cudaDeviceGetAttribute");
     }
-    if (!g_ready[dev][idx]) {
-      ce = cudaFuncSetAttribute(e.bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(e.bulk_smem));
-      if (ce != cudaSuccess) return fail(ce, "cudaFuncSetAttribute");
-      g_ready[dev][idx] = 1;
-    }
   }
   const int sms = g_sms[dev];
+  if (bulk) return launch_dmma<T>(stream, dev, sms, probs, nprob, reinterpret_cast<unsigned*>(ws) + 1);
 
+  int idx = -1;
+  for (int i = 0; i < kTsmmCount; ++i)
+    if (kTsmm[i].dtype == dtype && kTsmm[i].cap == cap) idx = i;
+  if (idx < 0) return TSM_ERROR_UNSUPPORTED;
   TsmmArgs<T> a{};
   a.nprob = nprob;
   a.error = reinterpret_cast<unsigned*>(ws) + 1;
   for (int i = 0; i < nprob; ++i) a.prob[i] = probs[i];
-  cudaError_t le;
-  if (bulk) {
-    int64_t total = 0;
-    for (int i = 0; i < nprob; ++i) {
-      TsmmProblem<T>& pr = a.prob[i];
-      pr.rows_main = tsmm_bulk_rows(pr.n, pr.p, sizeof(T));
-      pr.num_chunks = (pr.rows_main + e.rows - 1) / e.rows;
-      if (i == 0) a.split = pr.num_chunks;
-      total += pr.num_chunks;
-    }
-    if (nprob == 1) a.split = total;
-    a.total_chunks = total;
-    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(total, sms));
-    void* args[] = {&a};
-    le = cudaLaunchKernel(e.bulk, dim3(static_cast<unsigned>(grid)), dim3(e.bulk_threads), args, e.bulk_smem,
-                          stream);
-  } else {
-    int64_t nmax = 0;
-    for (int i = 0; i < nprob; ++i) nmax = std::max(nmax, a.prob[i].n);
-    const int rgn = cap >= 32 ? (8 / (cap / 32)) : 8 * (32 / cap);
-    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nmax + rgn - 1) / rgn, int64_t(sms) * 8));
-    void* args[] = {&a};
-    le = cudaLaunchKernel(e.direct, dim3(static_cast<unsigned>(grid)), dim3(256), args, 0, stream);
-  }
+  int64_t nmax = 0;
+  for (int i = 0; i < nprob; ++i) nmax = std::max(nmax, a.prob[i].n);
+  const int rgn = cap >= 32 ? (8 / (cap / 32)) : 8 * (32 / cap);
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((nmax + rgn - 1) / rgn, int64_t(sms) * 8));
+  void* args[] = {&a};
+  const cudaError_t le = cudaLaunchKernel(kTsmm[idx].direct, dim3(static_cast<unsigned>(grid)), dim3(256), args, 0, stream);
   if (le != cudaSuccess) return fail(le, "cudaLaunchKernel(tsmm)");
   return TSM_SUCCESS;
 }
