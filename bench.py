@@ -213,6 +213,28 @@ def _time(fn, reps: int, warmup: int = 3) -> float:
     return e0.elapsed_time(e1) / reps
 
 
+def fp64_gemm_peak(dev) -> dict:
+    """FP64 compute roof for the wide shapes: cuBLAS DGEMM (torch.matmul,
+    8192^3, 2 N^3 flops), best of 5 after one warm-up, CUDA events."""
+    import torch
+    n = 8192
+    a = torch.rand((n, n), dtype=torch.float64, device=dev)
+    b = torch.rand((n, n), dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    torch.cuda.empty_cache()
+    return {"tflops": round(2.0 * n**3 / (best * 1e-3) / 1e12, 2), "source": "cuBLAS DGEMM 8192^3 in this run"}
+
+
 def forms(dev) -> dict:
     """The three forms beside the plain FP64 path, each against FP64 on the
     same GPU: split precision (n = 2^25, m = k = 32, FP32 storage, column
@@ -434,7 +456,9 @@ def main() -> int:
 
     # ---------------- by width (each shape: warmup + timed launches)
     by_width = []
+    fp64_peak = None
     if not args.no_sweep and world == 1:
+        fp64_peak = fp64_gemm_peak(dev)
         for n, m, k in SWEEP:
             a, b = views(n, m, k)
             c = torch.zeros((m, k), dtype=torch.float64, device=dev)
@@ -450,9 +474,15 @@ def main() -> int:
             ms = e0.elapsed_time(e1) / args.sweep_steps
             gbs = algo_bytes(n, m, k) / (ms * 1e-3) / 1e9
             vi = lib.tsm_gemm_tn_default_variant(0, n, m, k, a.data_ptr(), m, b.data_ptr(), k)
+            # the binding roof: HBM bytes at the measured copy rate, or FP64
+            # FMAs at the measured DGEMM rate, whichever takes longer
+            t_hbm = algo_bytes(n, m, k) / (peaks["hbm_gbs"] * 1e9)
+            t_fp64 = 2.0 * n * m * k / (fp64_peak["tflops"] * 1e12)
             by_width.append({"n": n, "m": m, "k": k, "ms": round(ms, 4), "GB/s": round(gbs, 1),
                              "frac_hbm": round(gbs / peaks["hbm_gbs"], 4),
                              "GFLOP/s": round(2.0 * n * m * k / (ms * 1e-3) / 1e9, 1),
+                             "bound": "hbm" if t_hbm >= t_fp64 else "fp64",
+                             "frac_roof": round(max(t_hbm, t_fp64) / (ms * 1e-3), 4),
                              "variant": tsm.variants()[vi]["name"] if vi >= 0 else None})
 
     # ---------------- e2e through the C ABI from pinned host buffers
@@ -503,6 +533,7 @@ def main() -> int:
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(world),
                 "frac_hbm": value / world / peaks["hbm_gbs"], "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks, "by_width": by_width,
+                "fp64_peak": fp64_peak,
                 "checksum_ok": checksum_ok, "device_error_bits": dev_err, "forms": forms_out}
         print(json.dumps(line), flush=True)
     if world > 1:

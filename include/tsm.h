@@ -118,7 +118,7 @@ int tsm_gemm_tn_default_variant(int dtype, int64_t n, int m, int k, const void* 
 
 typedef struct tsm_variant_info {
   char name[64];
-  int kind;    /* 0 = TMA bulk pipeline, 1 = direct loads */
+  int kind;    /* 0 = TMA bulk pipeline, 1 = direct loads, 2 = FP64 tensor cores (2-D TMA) */
   int dtype;   /* TSM_F64 or TSM_F32 */
   int wa, wb;  /* widths (exact) or width capacities */
   int ta, tb;  /* per-thread tile of C */

@@ -143,6 +143,9 @@ def check(status: int, what: str = "") -> None:
     raise TsmError(status, f"{what}: {STATUS.get(status, status)}: {msg}" if what else msg)
 
 
+_KINDS = {0: "bulk", 1: "direct", 2: "dmma"}
+
+
 def variants() -> list[dict]:
     """All compiled variants, in table order."""
     lib = load()
@@ -150,7 +153,7 @@ def variants() -> list[dict]:
     for i in range(lib.tsm_variant_count()):
         info = VariantInfo()
         check(lib.tsm_variant_get_info(i, ctypes.byref(info)), "tsm_variant_get_info")
-        out.append(dict(index=i, name=info.name.decode(), kind="bulk" if info.kind == 0 else "direct",
+        out.append(dict(index=i, name=info.name.decode(), kind=_KINDS.get(info.kind, str(info.kind)),
                         dtype="f64" if info.dtype == 0 else "f32",
                         wa=info.wa, wb=info.wb, ta=info.ta, tb=info.tb, exact=bool(info.exact),
                         threads=info.threads, stages=info.stages, rows=info.rows, unroll=info.unroll,

@@ -41,13 +41,15 @@ def _cap(w: int) -> int:
     return c
 
 
-def candidates(variants: list[dict], m: int, k: int) -> list[dict]:
-    """Variants that accept (m, k): every exact one, and the capacity ones
-    no more than twice the smallest capacity per side (larger ones only add
-    masked work)."""
+def candidates(variants: list[dict], m: int, k: int, dtype: str = "f64") -> list[dict]:
+    """Variants of `dtype` that accept (m, k): every exact one, and the
+    capacity ones no more than twice the smallest capacity per side (larger
+    ones only add masked work)."""
     out = []
     cm, ck = _cap(m), _cap(k)
     for v in variants:
+        if v["dtype"] != dtype:
+            continue
         if v["exact"]:
             if m == v["wa"] and k == v["wb"]:
                 out.append(v)

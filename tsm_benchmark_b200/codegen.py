@@ -6,7 +6,8 @@ sycl_codegen_new.py:142-363).  Those emit one SYCL kernel per
 (M, N, TM, TN, stride, local_size, leap_frog, reduction, unroll) with scalar
 accumulators, a grid-stride row loop and FP64 atomics.  This generator emits
 rows of the kernel table in ``csrc/generated/``: explicit instantiations of
-the sm_100a templates in ``csrc/tsm_plain.cuh`` over the axes
+the sm_100a templates in ``csrc/tsm_plain.cuh`` (SIMT register tiles) and
+``csrc/tsm_dmma.cuh`` (FP64 tensor cores, exact widths 16..64) over the axes
 
     width pair      (wa, wb)        -- exact widths or width capacities
     tile            (ta, tb)        -- per-thread register tile of C
@@ -40,6 +41,7 @@ from __future__ import annotations
 import argparse
 import dataclasses
 import json
+import math
 import os
 import sys
 from typing import Iterable
@@ -182,6 +184,102 @@ class DirectVariant:
                 f'{self.tb}, {self.threads}, {"true" if self.exact else "false"})')
 
 
+@dataclasses.dataclass(frozen=True)
+class DmmaVariant:
+    """One FP64 tensor-core kernel (tsm_tn_dmma_kernel, csrc/tsm_dmma.cuh):
+    exact widths, multiples of 16 up to 64; 2-D swizzled TMA loads."""
+
+    wa: int
+    wb: int
+    mt: int = 0      # 8x8 tiles of C per warp along m (0: best loads-per-DMMA ratio)
+    nt: int = 0      # ... along k
+    cw: int = 0      # 0: regions x row slots, 8..12 warps
+    stages: int = 0  # 0: as many ~64 KB stages as fit, at most 4
+    rows: int = 0    # 0: ~64 KB stages
+    dtype: str = "f64"
+    exact: bool = True
+
+    @staticmethod
+    def best_region(wa: int, wb: int) -> tuple[int, int]:
+        """(mt, nt): even tile counts dividing wa/8 and wb/8, at most 16 tiles,
+        maximising DMMAs per shared load (mt nt / (mt/2 + nt/2)); ties go to
+        the larger region, then to mt >= nt."""
+        best = None
+        for mt in range(2, wa // 8 + 1, 2):
+            for nt in range(2, wb // 8 + 1, 2):
+                if (wa // 8) % mt or (wb // 8) % nt or mt * nt > 16:
+                    continue
+                key = (mt * nt / (mt + nt), mt * nt, mt >= nt)
+                if best is None or key > best[0]:
+                    best = (key, mt, nt)
+        return best[1], best[2]
+
+    @property
+    def regions(self) -> int:
+        mt, nt = (self.mt, self.nt) if self.mt else self.best_region(self.wa, self.wb)
+        return ((self.wa // 8) // mt) * ((self.wb // 8) // nt)
+
+    def resolved(self) -> "DmmaVariant":
+        v = self
+        if not v.mt:
+            mt, nt = self.best_region(v.wa, v.wb)
+            v = dataclasses.replace(v, mt=mt, nt=nt)
+        if not v.cw:
+            r = v.regions
+            v = dataclasses.replace(v, cw=r * max(1, -(-8 // r)))
+        blocks = v.wa // 16 + v.wb // 16
+        if not v.rows:
+            # whole 8-row swizzle groups and an equal number of 4-row k-steps
+            # for every row slot
+            slots = v.cw // v.regions
+            unit = 8 * 4 * slots // math.gcd(8, 4 * slots)
+            v = dataclasses.replace(v, rows=max(unit, min(256, 512 // blocks) // unit * unit))
+        if not v.stages:
+            stage = blocks * v.rows * 128
+            v = dataclasses.replace(v, stages=max(2, min(4, (SMEM_LIMIT - 2048) // stage)))
+        return v
+
+    @property
+    def name(self) -> str:
+        v = self.resolved()
+        return f"dmma_{v.wa}x{v.wb}_t{8 * v.mt}x{8 * v.nt}_w{v.cw}_s{v.stages}_r{v.rows}"
+
+    def smem_bytes(self) -> int:
+        v = self.resolved()
+        slots = v.cw // v.regions
+        ring = v.stages * (v.wa // 16 + v.wb // 16) * v.rows * 128
+        red = slots * v.wa * v.wb * 8
+        return 1024 + (max(ring, red) + 127) // 128 * 128 + 2 * v.stages * 8 + 16
+
+    def validate(self) -> list[str]:
+        v = self.resolved()
+        errs = []
+        if v.wa % 16 or v.wb % 16 or not (16 <= v.wa <= 64 and 16 <= v.wb <= 64):
+            errs.append("widths must be multiples of 16 in 16..64")
+        if v.mt % 2 or v.nt % 2 or (v.wa // 8) % v.mt or (v.wb // 8) % v.nt or v.mt * v.nt > 16:
+            errs.append("region: even tile counts dividing the widths, at most 16 tiles")
+        if v.cw % v.regions:
+            errs.append("consumer warps must cover whole regions")
+        if v.cw > 12:
+            errs.append("more than 12 consumer warps (register cap)")
+        if v.rows % 8 or v.rows > 256:
+            errs.append("chunk rows: multiple of 8, at most 256")
+        if (v.rows // 4) % (v.cw // v.regions):
+            errs.append("chunk k-steps must split evenly over the row slots")
+        if v.dtype != "f64":
+            errs.append("FP64 only")
+        if self.smem_bytes() > SMEM_LIMIT:
+            errs.append(f"shared memory {self.smem_bytes()} above {SMEM_LIMIT}")
+        return errs
+
+    def emit(self) -> str:
+        v = self.resolved()
+        return f'TSM_DMMA_VARIANT("{self.name}", {v.wa}, {v.wb}, {v.mt}, {v.nt}, {v.cw}, {v.stages}, {v.rows})'
+
+
+DMMA_WIDTHS = (16, 32, 48, 64)
+
+
 def default_tile(w: int) -> int:
     """Per-thread tile extent for a width (capacity)."""
     return {1: 1, 2: 2, 4: 4, 8: 4, 16: 8, 32: 8, 64: 8}[w]
@@ -208,6 +306,11 @@ EXTRA_CANDIDATES: dict[tuple[int, int], list[dict]] = {
 
 def default_variants() -> list:
     out: list = []
+    # FP64 tensor-core kernels first: exact widths, contiguous or strided
+    # operands with 16-byte row pitches.
+    for wa in DMMA_WIDTHS:
+        for wb in DMMA_WIDTHS:
+            out.append(DmmaVariant(wa, wb))
     for wa, wb in EXACT_PAIRS:
         base = BulkVariant(wa, wb, default_tile(wa), default_tile(wb))
         out.append(base)

@@ -7,6 +7,8 @@ namespace tsm {
 
 extern const Variant kGenPart0[];
 const Variant kGenPart0[] = {
+    TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s3_r256", 16, 16, 2, 2, 8, 3, 256),
+    TSM_DMMA_VARIANT("dmma_48x16_t48x16_w8_s3_r128", 48, 16, 6, 2, 8, 3, 128),
     TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r2048_u1", double, 1, 1, 1, 1, 8, 6, 2048, 1, true),
     TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r512_u2", double, 4, 4, 4, 4, 8, 6, 512, 2, true),
     TSM_BULK_VARIANT("bulk_8x8_t2x8_w8_s6_r256_u1", double, 8, 8, 2, 8, 8, 6, 256, 1, true),
@@ -39,6 +41,6 @@ const Variant kGenPart0[] = {
     TSM_DIRECT_VARIANT("directf32_64x4_t8x4_th256_cap", float, 64, 4, 8, 4, 256, false),
 };
 extern const int kGenPart0Count;
-const int kGenPart0Count = 30;
+const int kGenPart0Count = 32;
 
 }  // namespace tsm

@@ -7,6 +7,8 @@ namespace tsm {
 
 extern const Variant kGenPart1[];
 const Variant kGenPart1[] = {
+    TSM_DMMA_VARIANT("dmma_16x32_t16x32_w8_s3_r160", 16, 32, 2, 4, 8, 3, 160),
+    TSM_DMMA_VARIANT("dmma_48x32_t48x16_w8_s3_r96", 48, 32, 6, 2, 8, 3, 96),
     TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r2048_u2", double, 1, 1, 1, 1, 8, 6, 2048, 2, true),
     TSM_BULK_VARIANT("bulk_4x8_t4x4_w8_s6_r256_u1", double, 4, 8, 4, 4, 8, 6, 256, 1, true),
     TSM_BULK_VARIANT("bulk_8x16_t4x8_w8_s6_r128_u1", double, 8, 16, 4, 8, 8, 6, 128, 1, true),
@@ -39,6 +41,6 @@ const Variant kGenPart1[] = {
     TSM_DIRECT_VARIANT("directf32_64x8_t8x4_th256_cap", float, 64, 8, 8, 4, 256, false),
 };
 extern const int kGenPart1Count;
-const int kGenPart1Count = 30;
+const int kGenPart1Count = 32;
 
 }  // namespace tsm

@@ -7,6 +7,8 @@ namespace tsm {
 
 extern const Variant kGenPart2[];
 const Variant kGenPart2[] = {
+    TSM_DMMA_VARIANT("dmma_16x48_t16x48_w8_s3_r128", 16, 48, 2, 6, 8, 3, 128),
+    TSM_DMMA_VARIANT("dmma_48x48_t48x16_w9_s4_r72", 48, 48, 6, 2, 9, 4, 72),
     TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r2048_u4", double, 1, 1, 1, 1, 8, 6, 2048, 4, true),
     TSM_BULK_VARIANT("bulk_4x16_t4x8_w8_s6_r128_u1", double, 4, 16, 4, 8, 8, 6, 128, 1, true),
     TSM_BULK_VARIANT("bulk_8x32_t4x8_w8_s6_r96_u1", double, 8, 32, 4, 8, 8, 6, 96, 1, true),
@@ -39,6 +41,6 @@ const Variant kGenPart2[] = {
     TSM_DIRECT_VARIANT("directf32_64x16_t8x8_th256_cap", float, 64, 16, 8, 8, 256, false),
 };
 extern const int kGenPart2Count;
-const int kGenPart2Count = 30;
+const int kGenPart2Count = 32;
 
 }  // namespace tsm

@@ -7,6 +7,8 @@ namespace tsm {
 
 extern const Variant kGenPart3[];
 const Variant kGenPart3[] = {
+    TSM_DMMA_VARIANT("dmma_16x64_t16x64_w8_s3_r96", 16, 64, 2, 8, 8, 3, 96),
+    TSM_DMMA_VARIANT("dmma_48x64_t16x64_w9_s3_r72", 48, 64, 2, 8, 9, 3, 72),
     TSM_BULK_VARIANT("bulk_1x64_t1x8_w8_s6_r32_u1", double, 1, 64, 1, 8, 8, 6, 32, 1, true),
     TSM_BULK_VARIANT("bulk_4x32_t4x8_w8_s6_r64_u1", double, 4, 32, 4, 8, 8, 6, 64, 1, true),
     TSM_BULK_VARIANT("bulk_16x4_t8x4_w8_s6_r128_u1", double, 16, 4, 8, 4, 8, 6, 128, 1, true),
@@ -39,6 +41,6 @@ const Variant kGenPart3[] = {
     TSM_DIRECT_VARIANT("directf32_64x32_t8x8_th256_cap", float, 64, 32, 8, 8, 256, false),
 };
 extern const int kGenPart3Count;
-const int kGenPart3Count = 30;
+const int kGenPart3Count = 32;
 
 }  // namespace tsm

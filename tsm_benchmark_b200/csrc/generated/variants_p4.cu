@@ -7,6 +7,8 @@ namespace tsm {
 
 extern const Variant kGenPart4[];
 const Variant kGenPart4[] = {
+    TSM_DMMA_VARIANT("dmma_32x16_t32x16_w8_s3_r160", 32, 16, 4, 2, 8, 3, 160),
+    TSM_DMMA_VARIANT("dmma_64x16_t64x16_w8_s3_r96", 64, 16, 8, 2, 8, 3, 96),
     TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r1024_u1", double, 2, 2, 2, 2, 8, 6, 1024, 1, true),
     TSM_BULK_VARIANT("bulk_8x4_t4x4_w8_s6_r256_u1", double, 8, 4, 4, 4, 8, 6, 256, 1, true),
     TSM_BULK_VARIANT("bulk_16x8_t8x4_w8_s6_r128_u1", double, 16, 8, 8, 4, 8, 6, 128, 1, true),
@@ -39,6 +41,6 @@ const Variant kGenPart4[] = {
     TSM_DIRECT_VARIANT("directf32_64x64_t8x8_th256_cap", float, 64, 64, 8, 8, 256, false),
 };
 extern const int kGenPart4Count;
-const int kGenPart4Count = 30;
+const int kGenPart4Count = 32;
 
 }  // namespace tsm

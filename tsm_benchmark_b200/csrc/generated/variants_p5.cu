@@ -7,6 +7,8 @@ namespace tsm {
 
 extern const Variant kGenPart5[];
 const Variant kGenPart5[] = {
+    TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s3_r128", 32, 32, 4, 4, 8, 3, 128),
+    TSM_DMMA_VARIANT("dmma_64x32_t32x32_w8_s3_r80", 64, 32, 4, 4, 8, 3, 80),
     TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r1024_u2", double, 2, 2, 2, 2, 8, 6, 1024, 2, true),
     TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s6_r256_u1", double, 8, 8, 4, 4, 8, 6, 256, 1, true),
     TSM_BULK_VARIANT("bulk_16x16_t8x8_w8_s6_r128_u1", double, 16, 16, 8, 8, 8, 6, 128, 1, true),
@@ -38,6 +40,6 @@ const Variant kGenPart5[] = {
     TSM_DIRECT_VARIANT("directf32_32x64_t8x8_th256_cap", float, 32, 64, 8, 8, 256, false),
 };
 extern const int kGenPart5Count;
-const int kGenPart5Count = 29;
+const int kGenPart5Count = 31;
 
 }  // namespace tsm

@@ -7,6 +7,8 @@ namespace tsm {
 
 extern const Variant kGenPart6[];
 const Variant kGenPart6[] = {
+    TSM_DMMA_VARIANT("dmma_32x48_t16x48_w8_s3_r96", 32, 48, 2, 6, 8, 3, 96),
+    TSM_DMMA_VARIANT("dmma_64x48_t64x16_w9_s3_r72", 64, 48, 8, 2, 9, 3, 72),
     TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r512_u1", double, 4, 4, 4, 4, 8, 6, 512, 1, true),
     TSM_BULK_VARIANT("bulk_8x8_t8x8_w8_s6_r256_u1", double, 8, 8, 8, 8, 8, 6, 256, 1, true),
     TSM_BULK_VARIANT("bulk_16x16_t4x4_w8_s6_r128_u1", double, 16, 16, 4, 4, 8, 6, 128, 1, true),
@@ -38,6 +40,6 @@ const Variant kGenPart6[] = {
     TSM_DIRECT_VARIANT("directf32_64x1_t8x1_th256_cap", float, 64, 1, 8, 1, 256, false),
 };
 extern const int kGenPart6Count;
-const int kGenPart6Count = 29;
+const int kGenPart6Count = 31;
 
 }  // namespace tsm

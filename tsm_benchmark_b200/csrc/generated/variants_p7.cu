@@ -7,6 +7,8 @@ namespace tsm {
 
 extern const Variant kGenPart7[];
 const Variant kGenPart7[] = {
+    TSM_DMMA_VARIANT("dmma_32x64_t32x32_w8_s3_r80", 32, 64, 4, 4, 8, 3, 80),
+    TSM_DMMA_VARIANT("dmma_64x64_t32x32_w8_s3_r64", 64, 64, 4, 4, 8, 3, 64),
     TSM_BULK_VARIANT("bulk_4x4_t2x2_w8_s6_r512_u1", double, 4, 4, 2, 2, 8, 6, 512, 1, true),
     TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s6_r256_u2", double, 8, 8, 4, 4, 8, 6, 256, 2, true),
     TSM_BULK_VARIANT("bulk_16x16_t4x8_w8_s6_r128_u1", double, 16, 16, 4, 8, 8, 6, 128, 1, true),
@@ -38,6 +40,6 @@ const Variant kGenPart7[] = {
     TSM_DIRECT_VARIANT("directf32_64x2_t8x2_th256_cap", float, 64, 2, 8, 2, 256, false),
 };
 extern const int kGenPart7Count;
-const int kGenPart7Count = 29;
+const int kGenPart7Count = 31;
 
 }  // namespace tsm

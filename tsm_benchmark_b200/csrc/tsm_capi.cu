@@ -1,8 +1,11 @@
 // tsm_capi.cu -- the C ABI (include/tsm.h): argument checks, variant choice,
 // grid sizing and launches for the plain FP64 path.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -91,7 +94,7 @@ tsm_status prepare_variant(DeviceState* st, int idx) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-bool applicable(const Variant* v, int dtype, int m, int k, const void* A, int64_t lda, const void* B,
+bool applicable(const Variant* v, int dtype, int64_t n, int m, int k, const void* A, int64_t lda, const void* B,
                 int64_t ldb) {
   if (v->dtype != dtype) return false;
   if (v->exact ? (m != v->wa || k != v->wb) : (m > v->wa || k > v->wb)) return false;
@@ -99,7 +102,54 @@ bool applicable(const Variant* v, int dtype, int m, int k, const void* A, int64_
     if (lda != m || ldb != k) return false;
     if (!aligned16(A) || !aligned16(B)) return false;
   }
+  if (v->kind == kKindDmma) {
+    // Tensor maps: 16-byte aligned bases and row pitches, 32-bit row
+    // coordinates.
+    if ((lda * 8) % 16 != 0 || (ldb * 8) % 16 != 0) return false;
+    if (!aligned16(A) || !aligned16(B)) return false;
+    if (n > static_cast<int64_t>(INT_MAX) - v->rows) return false;
+  }
   return true;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of a row-major FP64 operand (rows x width, pitch ld elements)
+// with boxes of 16 columns x `box_rows` rows and the 128-byte swizzle the
+// DMMA kernels read with.
+tsm_status encode_operand_map(CUtensorMap* map, const double* base, int64_t rows, int width, int64_t ld,
+                              int box_rows) {
+  auto enc = tensor_map_encoder();
+  if (enc == nullptr) {
+    g_last_cuda_error = "cuTensorMapEncodeTiled: entry point not available";
+    return TSM_ERROR_CUDA;
+  }
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(width), static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * sizeof(double)};
+  const cuuint32_t box[2] = {16u, static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), "cuTensorMapEncodeTiled: CUresult %d", static_cast<int>(r));
+    g_last_cuda_error = buf;
+    return TSM_ERROR_CUDA;
+  }
+  return TSM_SUCCESS;
 }
 
 // Generated: preferred variant per (m, k, n) from the tuning table.
@@ -129,7 +179,7 @@ int default_variant(int dtype, int64_t n, int m, int k, const void* A, int64_t l
     if (std::sscanf(kTunedDefaults[i], "%d %d %lld %95s", &tm, &tk, &nmin, name) != 4) continue;
     if (tm != m || tk != k || nmin > n || nmin < best_nmin) continue;
     const int idx = find_variant(name);
-    if (idx >= 0 && applicable(vs[idx], dtype, m, k, A, lda, B, ldb)) {
+    if (idx >= 0 && applicable(vs[idx], dtype, n, m, k, A, lda, B, ldb)) {
       best = idx;
       best_nmin = nmin;
     }
@@ -138,7 +188,7 @@ int default_variant(int dtype, int64_t n, int m, int k, const void* A, int64_t l
   // 2. Table order: the generator lists exact bulk variants first, then
   //    capacity bulk variants from the smallest capacity up, then direct ones.
   for (size_t i = 0; i < vs.size(); ++i)
-    if (applicable(vs[i], dtype, m, k, A, lda, B, ldb)) return static_cast<int>(i);
+    if (applicable(vs[i], dtype, n, m, k, A, lda, B, ldb)) return static_cast<int>(i);
   return -1;
 }
 
@@ -174,6 +224,51 @@ size_t workspace_bytes_for(int sms, int m, int k) {
   return kWsHeader + static_cast<size_t>(sms) * kMaxCtasPerSm * m * k * sizeof(double);
 }
 
+// Rows the main loop streams, chunk count and grid for variant v (p.n, p.m,
+// p.k set).  Bulk: 16-byte copies leave up to three final rows of an
+// odd-width operand to the reduction epilogue.  DMMA: the tensor maps
+// zero-fill past row n, so every row is streamed.
+template <typename T>
+int64_t plan_grid(const Variant* v, const DeviceState* st, int idx, PlainArgs<T>& p) {
+  const int64_t max_grid = static_cast<int64_t>(st->sms) * st->occupancy[idx];
+  if (v->kind == kKindBulk || v->kind == kKindDmma) {
+    p.rows_main = v->kind == kKindBulk ? bulk_rows(p.n, p.m, p.k, sizeof(T)) : p.n;
+    p.num_chunks = (p.rows_main + v->rows - 1) / v->rows;
+    return std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, max_grid));
+  }
+  p.rows_main = p.n;
+  p.num_chunks = 0;
+  const int tiles = (v->wa / v->ta) * (v->wb / v->tb);
+  const int64_t row_groups = v->threads / tiles;
+  return std::max<int64_t>(1, std::min<int64_t>((p.n + row_groups - 1) / row_groups, max_grid));
+}
+
+template <typename T>
+tsm_status launch_variant(const Variant* v, const PlainArgs<T>& p, int64_t grid, cudaStream_t stream) {
+  cudaError_t e;
+  if (v->kind == kKindDmma) {
+    if constexpr (sizeof(T) == 8) {
+      DmmaArgs d{};
+      d.p = p;
+      if (p.n > 0) {  // n = 0: no chunks, the maps are never read
+        tsm_status s = encode_operand_map(&d.ta, p.A, p.n, p.m, p.lda, v->rows);
+        if (s == TSM_SUCCESS) s = encode_operand_map(&d.tb, p.B, p.n, p.k, p.ldb, v->rows);
+        if (s != TSM_SUCCESS) return s;
+      }
+      void* args[] = {&d};
+      e = cudaLaunchKernel(v->kernel, dim3(static_cast<unsigned>(grid)), dim3(v->threads), args, v->smem, stream);
+    } else {
+      return TSM_ERROR_UNSUPPORTED;
+    }
+  } else {
+    PlainArgs<T> q = p;
+    void* args[] = {&q};
+    e = cudaLaunchKernel(v->kernel, dim3(static_cast<unsigned>(grid)), dim3(v->threads), args, v->smem, stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernel");
+  return TSM_SUCCESS;
+}
+
 template <typename T>
 tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const T* A, int64_t lda, const T* B,
                         int64_t ldb, T* C, int64_t ldc, int accumulate, void* ws, size_t ws_bytes, int variant) {
@@ -191,7 +286,7 @@ tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const T* A
   if (idx < 0) {
     idx = default_variant(dtype, n, m, k, A, lda, B, ldb);
     if (idx < 0) return TSM_ERROR_UNSUPPORTED;
-  } else if (idx >= static_cast<int>(vs.size()) || !applicable(vs[idx], dtype, m, k, A, lda, B, ldb)) {
+  } else if (idx >= static_cast<int>(vs.size()) || !applicable(vs[idx], dtype, n, m, k, A, lda, B, ldb)) {
     return TSM_ERROR_UNSUPPORTED;
   }
   if ((s = prepare_variant(st, idx)) != TSM_SUCCESS) return s;
@@ -213,27 +308,8 @@ tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const T* A
   p.error = reinterpret_cast<unsigned*>(base) + 1;
   p.partials = reinterpret_cast<double*>(base + kWsHeader);
 
-  const int64_t max_grid = static_cast<int64_t>(st->sms) * st->occupancy[idx];
-  int64_t grid = 1;
-  if (v->kind == kKindBulk) {
-    // 16-byte bulk copies: up to three final rows of an odd-width operand
-    // are left to the reduction epilogue.
-    p.rows_main = bulk_rows(n, m, k, sizeof(T));
-    p.num_chunks = (p.rows_main + v->rows - 1) / v->rows;
-    grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, max_grid));
-  } else {
-    p.rows_main = n;
-    p.num_chunks = 0;
-    const int tiles = (v->wa / v->ta) * (v->wb / v->tb);
-    const int64_t row_groups = v->threads / tiles;
-    grid = std::max<int64_t>(1, std::min<int64_t>((n + row_groups - 1) / row_groups, max_grid));
-  }
-
-  void* args[] = {&p};
-  cudaError_t e = cudaLaunchKernel(v->kernel, dim3(static_cast<unsigned>(grid)), dim3(v->threads), args, v->smem,
-                                   stream);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernel");
-  return TSM_SUCCESS;
+  const int64_t grid = plan_grid(v, st, idx, p);
+  return launch_variant(v, p, grid, stream);
 }
 
 // ----------------------------------------------------------------- fills
@@ -456,19 +532,7 @@ extern "C" tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, in
   p.ldb = ldb;
   p.ldc = ldc;
   p.accumulate = accumulate ? 1 : 0;
-  const int64_t max_grid = static_cast<int64_t>(st->sms) * st->occupancy[idx];
-  int64_t grid = 1;
-  if (v->kind == kKindBulk) {
-    p.rows_main = bulk_rows(n, m, k, sizeof(double));
-    p.num_chunks = (p.rows_main + v->rows - 1) / v->rows;
-    grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, max_grid));
-  } else {
-    p.rows_main = n;
-    p.num_chunks = 0;
-    const int tiles = (v->wa / v->ta) * (v->wb / v->tb);
-    const int64_t row_groups = v->threads / tiles;
-    grid = std::max<int64_t>(1, std::min<int64_t>((n + row_groups - 1) / row_groups, max_grid));
-  }
+  const int64_t grid = plan_grid(v, st, idx, p);
   const size_t need = kWsHeader + static_cast<size_t>(grid) * m * k * sizeof(double);
   if (need > kStaticScratchBytes) return TSM_ERROR_WORKSPACE;
 
@@ -480,8 +544,5 @@ extern "C" tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, in
   cudaStream_t cs = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(unsigned), cs);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(static scratch counter)");
-  void* args[] = {&p};
-  e = cudaLaunchKernel(v->kernel, dim3(static_cast<unsigned>(grid)), dim3(v->threads), args, v->smem, cs);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernel");
-  return TSM_SUCCESS;
+  return launch_variant(v, p, grid, cs);
 }

@@ -1,6 +1,7 @@
 // tsm_device.cuh -- device-side building blocks for the sm_100a kernels:
 // shared-memory addresses, mbarriers with bounded waits, 1-D TMA bulk copies
-// (cp.async.bulk, no multicast) and the global timer.
+// and 2-D tiled TMA loads (no multicast), tcgen05 helpers and the global
+// timer.
 //
 // Every wait here is bounded: after kWaitLimitNs of wall time the wait gives
 // up, the caller records TSM_DEV_ERR_TIMEOUT in the workspace's error word and
@@ -92,6 +93,24 @@ __device__ __forceinline__ void bulk_g2s_evict_first(void* dst, const void* src,
       "%4;" ::"r"(smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
       : "memory");
+}
+
+// 2-D tiled TMA load (no multicast) of the box at element coordinates
+// (x, y) of `tmap` into this CTA's shared memory, completing the box's bytes
+// on `bar`.  x * element size must be a multiple of 16 bytes; rows y beyond
+// the tensor are filled with zeros.  `tmap` is the generic address of a
+// CUtensorMap in kernel-parameter (__grid_constant__) or global memory.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar,
+                                            uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint "
+      "[%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tensormap(const void* tmap) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
 }
 
 __device__ __forceinline__ uint64_t policy_evict_first() {
@@ -196,6 +215,22 @@ __device__ __forceinline__ float to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
+}
+
+// ---------------------------------------------------------------- DMMA
+// FP64 tensor-core MMA (mma.sync m8n8k4 .f64; lane = 4 g + t holds A[g][t],
+// B[t][g] and D[g][2t], D[g][2t + 1]): D += A B.
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+// D = A B (the first k-step of an accumulator: C = 0, no zeroing moves).
+__device__ __forceinline__ void dmma_m8n8k4_first(double& d0, double& d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%4, %4};"
+      : "=d"(d0), "=d"(d1)
+      : "d"(a), "d"(b), "d"(0.0));
 }
 
 }  // namespace dev

@@ -137,6 +137,10 @@ __device__ __forceinline__ void unrotate_tile(ACC (&acc)[TA][TB], int rotA, int 
   }
 }
 
+template <typename T>
+__device__ __forceinline__ void finish_partials(const PlainArgs<T>& p, const double* red, int slots, int t,
+                                                int nthreads, unsigned* s_is_last);
+
 // Sums the per-thread tiles of one CTA into `red`, then into this CTA's slot
 // of the workspace; the last CTA then writes C.  `red` must hold
 // slots * m * k doubles.  Called by all threads of the CTA (nthreads), of
@@ -184,6 +188,19 @@ __device__ __forceinline__ void finish_tiles(const PlainArgs<T>& p, ACC (&acc_in
     }
   }
   __syncthreads();
+  finish_partials(p, red, slots, t, nthreads, s_is_last);
+}
+
+// Steps 3 and 4 of the reduction: the CTA's `slots` m x k FP64 partial sums
+// in `red` (shared memory, complete: the caller synchronised) are summed in
+// slot order into this CTA's workspace slot; the last CTA to arrive sums the
+// CTA partials in CTA order (plus the rows [rows_main, n) the main loop left)
+// and writes C.  Called by all `nthreads` threads of the CTA.
+template <typename T>
+__device__ __forceinline__ void finish_partials(const PlainArgs<T>& p, const double* red, int slots, int t,
+                                                int nthreads, unsigned* s_is_last) {
+  const int m = p.m, k = p.k;
+  const int mk = m * k;
   // 3. Fixed-order sum over the slots -> this CTA's partial in the workspace.
   double* mine = p.partials + static_cast<int64_t>(blockIdx.x) * mk;
   for (int e = t; e < mk; e += nthreads) {

@@ -10,11 +10,12 @@
 
 #include <cstddef>
 
+#include "tsm_dmma.cuh"
 #include "tsm_plain.cuh"
 
 namespace tsm {
 
-enum VariantKind : int { kKindBulk = 0, kKindDirect = 1 };
+enum VariantKind : int { kKindBulk = 0, kKindDirect = 1, kKindDmma = 2 };
 enum DType : int { kF64 = 0, kF32 = 1 };
 
 template <typename T>
@@ -33,7 +34,7 @@ struct Variant {
   int kind;     // VariantKind
   int dtype;    // DType of A, B and C
   int wa, wb;   // widths (exact) or capacities
-  int ta, tb;   // per-thread tile of C
+  int ta, tb;   // per-thread tile of C (DMMA: per-warp region of C)
   int exact;    // 1: only m == wa && k == wb; 0: any m <= wa, k <= wb
   int threads;  // CTA size
   int stages;   // bulk: shared-memory ring depth
@@ -67,4 +68,12 @@ extern const int kVariantPartCount;
     NAME, ::tsm::kKindDirect, ::tsm::DTypeOf<T>::value, WA, WB, TA, TB, EX, TH, 0, 0, 1,           \
         ::tsm::DirectKernel<T, WA, WB, TA, TB, TH, EX>::SMEM_BYTES,                                \
         reinterpret_cast<const void*>(&::tsm::tsm_tn_direct_kernel<T, WA, WB, TA, TB, TH, EX>)     \
+  }
+
+#define TSM_DMMA_VARIANT(NAME, WA, WB, MT, NT, CW, ST, RS)                                                 \
+  ::tsm::Variant {                                                                                         \
+    NAME, ::tsm::kKindDmma, ::tsm::kF64, WA, WB, MT * 8, NT * 8, 1,                                          \
+        ::tsm::DmmaTn<WA, WB, MT, NT, CW, ST, RS>::THREADS, ST, RS, 1,                                       \
+        ::tsm::DmmaTn<WA, WB, MT, NT, CW, ST, RS>::SMEM_BYTES,                                               \
+        reinterpret_cast<const void*>(&::tsm::tsm_tn_dmma_kernel<WA, WB, MT, NT, CW, ST, RS>)                \
   }

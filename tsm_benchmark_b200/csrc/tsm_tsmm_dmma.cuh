@@ -40,19 +40,6 @@
 
 namespace tsm {
 
-__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
-  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-      : "+d"(d0), "+d"(d1)
-      : "d"(a), "d"(b));
-}
-
-// D = A B (the first k-step of an accumulator: C = 0, no zeroing moves).
-__device__ __forceinline__ void dmma_m8n8k4_first(double& d0, double& d1, double a, double b) {
-  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%4, %4};"
-      : "=d"(d0), "=d"(d1)
-      : "d"(a), "d"(b), "d"(0.0));
-}
-
 template <typename TX, int P, int Q, int CW, int STAGES, int RS>
 struct TsmmDmmaKernel {
   static_assert(P >= 4 && P <= 64 && (P & (P - 1)) == 0, "P: power of two in 4..64");
@@ -241,9 +228,9 @@ __global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>::THRE
 #pragma unroll
                 for (int i = 0; i < K::RG; ++i) {
                   if (kb == 0 && e == 0)
-                    dmma_m8n8k4_first(d[i][j][0], d[i][j][1], a[i][e], b[K::KPL * kb + e][j]);
+                    dev::dmma_m8n8k4_first(d[i][j][0], d[i][j][1], a[i][e], b[K::KPL * kb + e][j]);
                   else
-                    dmma_m8n8k4(d[i][j][0], d[i][j][1], a[i][e], b[K::KPL * kb + e][j]);
+                    dev::dmma_m8n8k4(d[i][j][0], d[i][j][1], a[i][e], b[K::KPL * kb + e][j]);
                 }
           }
           if (Q >= 8 || 2 * t < Q) {
@@ -289,7 +276,7 @@ __global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>::THRE
             for (int j = 0; j < K::NT; ++j)
 #pragma unroll
               for (int i = 0; i < K::RG; ++i)
-                dmma_m8n8k4(d[i][j][0], d[i][j][1], a[i][e], b[K::KPL * kb + e][j]);
+                dev::dmma_m8n8k4(d[i][j][0], d[i][j][1], a[i][e], b[K::KPL * kb + e][j]);
         }
         // D[g][2t + {0,1}] of tile j -> Y[r][o0 + 8 j + 2 t + {0,1}]
 #pragma unroll
