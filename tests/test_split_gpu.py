@@ -26,8 +26,12 @@ def errors(ref, got, A, B):
     return nw, pe
 
 
+# Widths that are multiples of 4 take the 2-D TMA kernel (columns beyond the
+# width and rows beyond n zero-filled by the tensor maps); (5, 17) takes the
+# 1-D bulk kernel with its converter pass.
 @pytest.mark.parametrize("n,m,k", [(4096, 32, 32), (100003, 32, 32), (3, 32, 32), (0, 8, 8), (65539, 5, 17),
-                                   (20000, 32, 4), (1 << 20, 16, 16)])
+                                   (20000, 32, 4), (1 << 20, 16, 16), (70001, 8, 24), (129, 12, 28), (1, 4, 4),
+                                   (257, 32, 8), (33333, 3, 32)])
 def test_split_parity(gpu, oracle_mod, n, m, k):
     from tsm_benchmark_b200 import tsmttsm_split, workspace_status
     A = scaled_normal(n, m, n + m)

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/tsm.h"
+#include "tsm_errors.h"
 #include "tsm_batched.cuh"
 
 namespace tsm {
@@ -51,12 +52,11 @@ struct Schedule {
   int grid = 0;
 };
 
-thread_local std::string g_batched_error;
 
 tsm_status fail(cudaError_t e, const char* what) {
   char buf[256];
   std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
-  g_batched_error = buf;
+  last_error() = buf;
   return TSM_ERROR_CUDA;
 }
 

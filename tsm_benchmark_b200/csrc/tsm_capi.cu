@@ -1,8 +1,6 @@
 // tsm_capi.cu -- the C ABI (include/tsm.h): argument checks, variant choice,
 // grid sizing and launches for the plain FP64 path.
-#include <cuda.h>
 #include <cuda_runtime.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <climits>
@@ -15,12 +13,18 @@
 #include <vector>
 
 #include "../../include/tsm.h"
+#include "tsm_errors.h"
 #include "tsm_registry.cuh"
+#include "tsm_tmap.h"
 
 namespace tsm {
 namespace {
-
 thread_local std::string g_last_cuda_error;
+}  // namespace
+
+std::string& last_error() { return g_last_cuda_error; }
+
+namespace {
 
 tsm_status cuda_fail(cudaError_t e, const char* what) {
   char buf[256];
@@ -112,43 +116,14 @@ bool applicable(const Variant* v, int dtype, int64_t n, int m, int k, const void
   return true;
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
-// dependency on the driver library).
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      p = nullptr;
-    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }();
-  return fn;
-}
-
 // Tensor map of a row-major FP64 operand (rows x width, pitch ld elements)
 // with boxes of 16 columns x `box_rows` rows and the 128-byte swizzle the
 // DMMA kernels read with.
 tsm_status encode_operand_map(CUtensorMap* map, const double* base, int64_t rows, int width, int64_t ld,
                               int box_rows) {
-  auto enc = tensor_map_encoder();
-  if (enc == nullptr) {
-    g_last_cuda_error = "cuTensorMapEncodeTiled: entry point not available";
+  if (!encode_rowmajor_map(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, base, rows, width, ld, 16, box_rows,
+                           CU_TENSOR_MAP_SWIZZLE_128B, &g_last_cuda_error))
     return TSM_ERROR_CUDA;
-  }
-  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(width), static_cast<cuuint64_t>(rows)};
-  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * sizeof(double)};
-  const cuuint32_t box[2] = {16u, static_cast<cuuint32_t>(box_rows)};
-  const cuuint32_t estr[2] = {1u, 1u};
-  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
-                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    char buf[96];
-    std::snprintf(buf, sizeof(buf), "cuTensorMapEncodeTiled: CUresult %d", static_cast<int>(r));
-    g_last_cuda_error = buf;
-    return TSM_ERROR_CUDA;
-  }
   return TSM_SUCCESS;
 }
 

@@ -1,15 +1,21 @@
 // tsm_split.cu -- C ABI of the precision form (FP32 storage, TF32 hi/lo
-// split on tcgen05 tensor cores, FP64 reductions).  Kernel: tsm_split.cuh.
+// split on tcgen05 tensor cores, FP64 reductions).  Kernels: tsm_split_tma.cuh
+// (widths that are multiples of 4: 2-D TMA straight into the MMA layout) and
+// tsm_split.cuh (any width: 1-D bulk copies and a converter pass).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
 #include <string>
 
 #include "../../include/tsm.h"
+#include "tsm_errors.h"
 #include "tsm_split.cuh"
+#include "tsm_split_tma.cuh"
+#include "tsm_tmap.h"
 
 namespace tsm {
 namespace {
@@ -17,12 +23,12 @@ namespace {
 std::mutex g_split_mu;
 int g_split_sms[64] = {};
 bool g_split_attr[64] = {};
-thread_local std::string g_split_error;
+bool g_split_tma_attr[64] = {};
 
 tsm_status split_fail(cudaError_t e, const char* what) {
   char buf[256];
   std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
-  g_split_error = buf;
+  last_error() = buf;
   return TSM_ERROR_CUDA;
 }
 
@@ -74,6 +80,8 @@ extern "C" tsm_status tsm_gemm_tn_f32_split(tsm_stream_t stream, int64_t n, int 
   const int sms = g_split_sms[dev];
   const size_t need = 256 + static_cast<size_t>(sms) * 4 * m * k * sizeof(double);
   if (workspace == nullptr || workspace_bytes < need || !aligned16(workspace)) return TSM_ERROR_WORKSPACE;
+  // Widths that are multiples of 4 floats (16-byte row pitches): tensor maps.
+  const bool tma = m % 4 == 0 && k % 4 == 0 && n <= static_cast<int64_t>(INT_MAX) - split2::kRows;
   SplitArgs p{};
   p.A = A;
   p.B = B;
@@ -83,12 +91,41 @@ extern "C" tsm_status tsm_gemm_tn_f32_split(tsm_stream_t stream, int64_t n, int 
   p.k = k;
   p.ldc = ldc;
   p.accumulate = accumulate ? 1 : 0;
-  p.rows_main = rows_for_bulk(n, m, k);
-  p.num_chunks = (p.rows_main + split::kRows - 1) / split::kRows;
   unsigned char* base = static_cast<unsigned char*>(workspace);
   p.counter = reinterpret_cast<unsigned*>(base);
   p.error = reinterpret_cast<unsigned*>(base) + 1;
   p.partials = reinterpret_cast<double*>(base + 256);
+  if (tma) {
+    {
+      std::lock_guard<std::mutex> lk(g_split_mu);
+      if (!g_split_tma_attr[dev]) {
+        e = cudaFuncSetAttribute(reinterpret_cast<const void*>(&tsm_tn_split_tf32_tma_kernel),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(split2::kSmemBytes));
+        if (e != cudaSuccess) return split_fail(e, "cudaFuncSetAttribute(split tma)");
+        g_split_tma_attr[dev] = true;
+      }
+    }
+    SplitTmaArgs a{};
+    p.rows_main = n;  // the tensor maps zero-fill past row n
+    p.num_chunks = (n + split2::kRows - 1) / split2::kRows;
+    a.p = p;
+    if (n > 0) {  // n = 0: no chunks, the maps are never read
+      if (!encode_rowmajor_map(&a.ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, n, m, lda, 32, split2::kRows,
+                               CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, &last_error()) ||
+          !encode_rowmajor_map(&a.tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, B, n, k, ldb, 32, split2::kRows,
+                               CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, &last_error()))
+        return TSM_ERROR_CUDA;
+    }
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, sms));
+    void* args[] = {&a};
+    e = cudaLaunchKernel(reinterpret_cast<const void*>(&tsm_tn_split_tf32_tma_kernel),
+                         dim3(static_cast<unsigned>(grid)), dim3(split2::kThreads), args, split2::kSmemBytes,
+                         static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return split_fail(e, "cudaLaunchKernel(split tma)");
+    return TSM_SUCCESS;
+  }
+  p.rows_main = rows_for_bulk(n, m, k);
+  p.num_chunks = (p.rows_main + split::kRows - 1) / split::kRows;
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, sms));
   void* args[] = {&p};
   e = cudaLaunchKernel(reinterpret_cast<const void*>(&tsm_tn_split_tf32_kernel), dim3(static_cast<unsigned>(grid)),

@@ -86,6 +86,53 @@ __device__ __forceinline__ uint32_t op_offset(int r, int c) {
 
 }  // namespace split
 
+// The end of both split kernels: the epilogue warps' FP64 sums (warps
+// epi0..epi0+3, lanes 0-15: D row 16 (w % 4) + lane, 32 columns) -> `red`
+// (16 KB of shared memory no longer in use), the CTA's m x k partial (D rows
+// i and 32 + i -- the hi and lo parts of A's column i -- added) into the
+// workspace, and the last CTA's fixed-order sum over CTAs (plus the rows
+// [rows_main, n) the pipeline left) into C.
+__device__ __forceinline__ void split_finish(const SplitArgs& p, const double (&acc)[32], double* red, int t,
+                                             int nthreads, int epi0, unsigned* s_is_last) {
+  const int warp = t >> 5, lane = t & 31;
+  const int m = p.m, k = p.k;
+  if (warp >= epi0 && warp < epi0 + 4 && lane < 16) {
+    const int q = warp & 3;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) red[(q * 16 + lane) * 32 + j] = acc[j];
+  }
+  __syncthreads();
+  const int mk = m * k;
+  double* mine = p.partials + static_cast<int64_t>(blockIdx.x) * mk;
+  for (int e = t; e < mk; e += nthreads) {
+    const int i = e / k, j = e - (e / k) * k;
+    // row i of C: hi part in D row i (sub-partition i / 16), lo part in row 32 + i.
+    const int hi_slot = (i >> 4) * 16 + (i & 15);
+    const int lo_slot = (2 + (i >> 4)) * 16 + (i & 15);
+    mine[e] = red[hi_slot * 32 + j] + red[lo_slot * 32 + j];
+  }
+  __threadfence();
+  __syncthreads();
+  if (t == 0) {
+    const unsigned prev = atomicAdd(p.counter, 1u);
+    *s_is_last = (prev == gridDim.x - 1) ? 1u : 0u;
+  }
+  __syncthreads();
+  if (*s_is_last == 0u) return;
+  __threadfence();
+  const int64_t G = gridDim.x;
+  for (int e = t; e < mk; e += nthreads) {
+    const int i = e / k, j = e - (e / k) * k;
+    double s = dev::ld_cg(p.partials + e);
+    for (int64_t b = 1; b < G; ++b) s += dev::ld_cg(p.partials + b * mk + e);
+    for (int64_t r = p.rows_main; r < p.n; ++r)
+      s += static_cast<double>(p.A[r * m + i]) * static_cast<double>(p.B[r * k + j]);
+    double* c = p.C + static_cast<int64_t>(i) * p.ldc + j;
+    *c = p.accumulate ? *c + s : s;
+  }
+  if (t == 0) *p.counter = 0u;
+}
+
 __global__ void __launch_bounds__(split::kThreads, 1) tsm_tn_split_tf32_kernel(const SplitArgs p) {
   using namespace split;
   extern __shared__ unsigned char smem_raw[];
@@ -314,42 +361,7 @@ __global__ void __launch_bounds__(split::kThreads, 1) tsm_tn_split_tf32_kernel(c
   dev::tc_fence_after();
   if (warp == 1) dev::tmem_dealloc(tmem, kTmemCols);
 
-  // ---------------- CTA reduction (FP64, fixed order) and the last CTA's sum.
-  double* red = reinterpret_cast<double*>(raw_ring);  // 4 warps x 16 lanes x 32 doubles = 16 KB
-  if (warp >= kEpiWarp0 && lane < 16) {
-    const int q = warp & 3;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) red[(q * 16 + lane) * 32 + j] = acc[j];
-  }
-  __syncthreads();
-  const int mk = m * k;
-  double* mine = p.partials + static_cast<int64_t>(blockIdx.x) * mk;
-  for (int e = t; e < mk; e += kThreads) {
-    const int i = e / k, j = e - (e / k) * k;
-    // row i of C: hi part in D row i (sub-partition i / 16), lo part in row 32 + i.
-    const int hi_slot = (i >> 4) * 16 + (i & 15);
-    const int lo_slot = (2 + (i >> 4)) * 16 + (i & 15);
-    mine[e] = red[hi_slot * 32 + j] + red[lo_slot * 32 + j];
-  }
-  __threadfence();
-  __syncthreads();
-  if (t == 0) {
-    const unsigned prev = atomicAdd(p.counter, 1u);
-    *s_is_last = (prev == gridDim.x - 1) ? 1u : 0u;
-  }
-  __syncthreads();
-  if (*s_is_last == 0u) return;
-  __threadfence();
-  for (int e = t; e < mk; e += kThreads) {
-    const int i = e / k, j = e - (e / k) * k;
-    double s = dev::ld_cg(p.partials + e);
-    for (int b = 1; b < G; ++b) s += dev::ld_cg(p.partials + static_cast<int64_t>(b) * mk + e);
-    for (int64_t r = p.rows_main; r < p.n; ++r)
-      s += static_cast<double>(p.A[r * m + i]) * static_cast<double>(p.B[r * k + j]);
-    double* c = p.C + static_cast<int64_t>(i) * p.ldc + j;
-    *c = p.accumulate ? *c + s : s;
-  }
-  if (t == 0) *p.counter = 0u;
+  split_finish(p, acc, reinterpret_cast<double*>(raw_ring), t, kThreads, kEpiWarp0, s_is_last);
 }
 
 }  // namespace tsm

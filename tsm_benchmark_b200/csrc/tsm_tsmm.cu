@@ -9,6 +9,7 @@
 #include <string>
 
 #include "../../include/tsm.h"
+#include "tsm_errors.h"
 #include "tsm_tsmm.cuh"
 #include "tsm_tsmm_dmma.cuh"
 
@@ -70,7 +71,6 @@ const DmmaEntry kDmma[] = {
 };
 constexpr int kDmmaCount = sizeof(kDmma) / sizeof(kDmma[0]);
 
-thread_local std::string g_tsmm_error;
 std::mutex g_tsmm_mu;
 int g_sms[64] = {};
 signed char g_dmma_ready[64][kDmmaCount] = {};
@@ -78,7 +78,7 @@ signed char g_dmma_ready[64][kDmmaCount] = {};
 tsm_status fail(cudaError_t e, const char* what) {
   char buf[256];
   std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
-  g_tsmm_error = buf;
+  last_error() = buf;
   return TSM_ERROR_CUDA;
 }
 
