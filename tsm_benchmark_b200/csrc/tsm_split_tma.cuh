@@ -17,8 +17,12 @@
 //     exact), elementwise at the same offset of a parallel tile: no address
 //     arithmetic, 16-byte loads and stores, integer rounding (no conversion
 //     instructions).  |x - hi - lo| <= 2^-21 |x|.
-// Stage layout (64 KB, 1024-byte aligned): A_hi | B_hi | A_lo | B_lo, 16 KB
-// each, so an operand's lo atoms sit LBO = 32 KB after its hi atoms.
+// Shared memory: a ring of hi stages (A_hi | B_hi, 16 KB each) that the TMA
+// unit fills -- a stage stays busy until its MMAs complete, so its depth is
+// what keeps bytes in flight -- and, after it, a shallower ring of lo stages
+// (A_lo | B_lo).  Each chunk's descriptors carry the distance from its hi
+// stage to its lo stage as the leading byte offset (LBO) between the hi and
+// lo atoms of an operand.
 //
 // Warp roles (14 warps): 0 producer, 1 TMEM owner + MMA issuer, 2-9
 // converters, 10-13 epilogue (TMEM -> FP64 sums, double-buffered
@@ -45,21 +49,23 @@ struct SplitTmaArgs {
 namespace split2 {
 
 constexpr int kRows = 128;                   // rows per chunk (16 MMAs of K = 8)
-constexpr int kStages = 3;
+constexpr int kHiStages = 5;
+constexpr int kLoStages = 2;
 constexpr int kTileBytes = kRows * 128;      // one operand part: 32 floats x 128 rows
-constexpr int kLoOffset = 2 * kTileBytes;    // hi -> lo distance (the descriptors' LBO)
-constexpr int kStageBytes = 4 * kTileBytes;  // A hi, B hi, A lo, B lo
+constexpr int kStageBytes = 2 * kTileBytes;  // A part, B part
+constexpr int kLoRing = kHiStages * kStageBytes;  // offset of the lo ring
 constexpr int kConvWarps = 8;
 constexpr int kEpiWarp0 = 10;
 constexpr int kWarps = 14;
 constexpr int kThreads = kWarps * 32;
 constexpr int kTmemCols = 128;  // two 64-column accumulators
 constexpr uint32_t kIdesc = dev::umma_idesc_tf32(64, 64, true, true);
-constexpr size_t kBarOffset = size_t(kStages) * kStageBytes;
-constexpr int kNumBars = 3 * kStages + 4;
+constexpr size_t kBarOffset = size_t(kLoRing) + size_t(kLoStages) * kStageBytes;
+constexpr int kNumBars = 2 * kHiStages + 2 * kLoStages + 4;
 constexpr size_t kSmemBytes = kBarOffset + kNumBars * 8 + 32 + 1024;  // + alignment slack
 static_assert(kTileBytes % 1024 == 0, "tiles keep the 1024-byte alignment of the swizzle atoms");
-static_assert(kLoOffset / 16 < (1 << 14), "LBO must fit the descriptor field");
+static_assert((kLoRing + (kLoStages - 1) * kStageBytes) / 16 < (1 << 14), "LBO must fit the descriptor field");
+static_assert(kSmemBytes <= 232448, "dynamic shared memory limit of sm_100a");
 
 // lo part of x: x - trunc_tf32(x) (exact) rounded to nearest TF32, ties away
 // from zero (add half a TF32 unit to the magnitude bits, clear 13 bits).
@@ -79,11 +85,12 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((1024u - (dev::smem_u32(smem_raw) & 1023u)) & 1023u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBarOffset);
-  uint64_t* full = bars;                // hi tiles landed (TMA transaction count)
-  uint64_t* lo_full = full + kStages;   // lo tiles written (converter warps)
-  uint64_t* empty = lo_full + kStages;  // the stage's MMAs completed (commit)
-  uint64_t* d_full = empty + kStages;   // accumulator b complete (commit)
-  uint64_t* d_empty = d_full + 2;       // accumulator b drained (epilogue warps)
+  uint64_t* full = bars;                     // hi stage landed (TMA transaction count)
+  uint64_t* empty = full + kHiStages;        // hi stage's MMAs completed (commit)
+  uint64_t* lo_full = empty + kHiStages;     // lo stage written (converter warps)
+  uint64_t* lo_empty = lo_full + kLoStages;  // lo stage's MMAs completed (commit)
+  uint64_t* d_full = lo_empty + kLoStages;   // accumulator b complete (commit)
+  uint64_t* d_empty = d_full + 2;            // accumulator b drained (epilogue warps)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kNumBars);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
   unsigned* s_is_last = reinterpret_cast<unsigned*>(tmem_slot + 2);
@@ -93,10 +100,13 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
   const int64_t G = gridDim.x;
 
   if (t == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < kHiStages; ++s) {
       dev::mbar_init(&full[s], 1);
-      dev::mbar_init(&lo_full[s], kConvWarps);
       dev::mbar_init(&empty[s], 1);
+    }
+    for (int o = 0; o < kLoStages; ++o) {
+      dev::mbar_init(&lo_full[o], kConvWarps);
+      dev::mbar_init(&lo_empty[o], 1);
     }
     for (int b = 0; b < 2; ++b) {
       dev::mbar_init(&d_full[b], 1);
@@ -129,10 +139,11 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
     }
     const uint64_t policy = dev::policy_evict_first();
     for (int64_t it = 0; it < nchunks_mine; ++it) {
-      const int s = static_cast<int>(it % kStages);
+      const int s = static_cast<int>(it % kHiStages);
       bool ok = true;
       if (lane == 0) {
-        if (it >= kStages) ok = dev::mbar_wait(&empty[s], static_cast<uint32_t>(((it / kStages) - 1) & 1), abort);
+        if (it >= kHiStages)
+          ok = dev::mbar_wait(&empty[s], static_cast<uint32_t>(((it / kHiStages) - 1) & 1), abort);
         if (ok) {
           unsigned char* st = smem + s * kStageBytes;
           const int y = static_cast<int>((blockIdx.x + it * G) * kRows);
@@ -151,23 +162,26 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
     // ---------------- MMA issuer (lane 0); the warp stays converged.
     const uint32_t base = dev::smem_u32(smem);
     for (int64_t it = 0; it < nchunks_mine; ++it) {
-      const int s = static_cast<int>(it % kStages);
+      const int s = static_cast<int>(it % kHiStages);
+      const int o = static_cast<int>(it % kLoStages);
       const int b = static_cast<int>(it & 1);
       bool ok = true;
       if (lane == 0) {
-        ok = dev::mbar_wait(&lo_full[s], static_cast<uint32_t>((it / kStages) & 1), abort);
+        ok = dev::mbar_wait(&lo_full[o], static_cast<uint32_t>((it / kLoStages) & 1), abort);
         if (ok && it >= 2) ok = dev::mbar_wait(&d_empty[b], static_cast<uint32_t>(((it >> 1) - 1) & 1), abort);
         if (ok) {
           dev::tc_fence_after();
           const uint32_t a_base = base + s * kStageBytes;
           const uint32_t b_base = a_base + kTileBytes;
+          const uint32_t lbo = static_cast<uint32_t>(kLoRing + o * kStageBytes - s * kStageBytes);  // hi -> lo
 #pragma unroll
           for (int g = 0; g < kRows / 8; ++g) {
-            const uint64_t ad = dev::umma_smem_desc(a_base + g * 1024, kLoOffset, split::kSbo, split::kLayout);
-            const uint64_t bd = dev::umma_smem_desc(b_base + g * 1024, kLoOffset, split::kSbo, split::kLayout);
+            const uint64_t ad = dev::umma_smem_desc(a_base + g * 1024, lbo, split::kSbo, split::kLayout);
+            const uint64_t bd = dev::umma_smem_desc(b_base + g * 1024, lbo, split::kSbo, split::kLayout);
             dev::umma_tf32(tmem + b * 64, ad, bd, kIdesc, g > 0 ? 1u : 0u);
           }
-          dev::umma_commit(&empty[s]);  // the stage may be refilled once these MMAs are done
+          dev::umma_commit(&empty[s]);     // the hi stage may be refilled once these MMAs are done
+          dev::umma_commit(&lo_empty[o]);  // and the lo stage rewritten
           dev::umma_commit(&d_full[b]);
         } else {
           *abort = 1;
@@ -181,14 +195,18 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
     // ---------------- converters: lo parts, elementwise at the hi offsets
     const int ct = t - 64;  // 0 .. 255
     for (int64_t it = 0; it < nchunks_mine; ++it) {
-      const int s = static_cast<int>(it % kStages);
-      if (!dev::mbar_wait(&full[s], static_cast<uint32_t>((it / kStages) & 1), abort)) {
+      const int s = static_cast<int>(it % kHiStages);
+      const int o = static_cast<int>(it % kLoStages);
+      bool ok = dev::mbar_wait(&full[s], static_cast<uint32_t>((it / kHiStages) & 1), abort);
+      if (ok && it >= kLoStages)
+        ok = dev::mbar_wait(&lo_empty[o], static_cast<uint32_t>(((it / kLoStages) - 1) & 1), abort);
+      if (!ok) {
         *abort = 1;
         atomicOr(p.error, dev::kErrTimeout);
         break;
       }
       const uint4* hi = reinterpret_cast<const uint4*>(smem + s * kStageBytes);
-      uint4* lo = reinterpret_cast<uint4*>(smem + s * kStageBytes + kLoOffset);
+      uint4* lo = reinterpret_cast<uint4*>(smem + kLoRing + o * kStageBytes);
       // A_hi and B_hi: 2 x 16 KB = 2048 16-byte vectors over 256 threads.
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
@@ -202,7 +220,7 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       }
       dev::fence_proxy_async_smem();  // make the lo tiles visible to the tensor core
       __syncwarp();
-      if (lane == 0) dev::mbar_arrive(&lo_full[s]);
+      if (lane == 0) dev::mbar_arrive(&lo_full[o]);
     }
   } else {
     // ---------------- epilogue: TMEM -> FP64 sums (lanes 0-15 of each warp)
@@ -240,8 +258,8 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
     // running (issuer).  A second timeout is only recorded.
     volatile int no_abort = 0;
     if (warp == 0) {
-      for (int64_t it = nchunks_mine > kStages ? nchunks_mine - kStages : 0; it < nchunks_mine; ++it)
-        if (!dev::mbar_wait(&full[it % kStages], static_cast<uint32_t>((it / kStages) & 1), &no_abort)) break;
+      for (int64_t it = nchunks_mine > kHiStages ? nchunks_mine - kHiStages : 0; it < nchunks_mine; ++it)
+        if (!dev::mbar_wait(&full[it % kHiStages], static_cast<uint32_t>((it / kHiStages) & 1), &no_abort)) break;
     } else if (warp == 1) {
       for (int64_t it = nchunks_mine > 2 ? nchunks_mine - 2 : 0; it < nchunks_mine; ++it)
         if (!dev::mbar_wait(&d_full[it & 1], static_cast<uint32_t>((it >> 1) & 1), &no_abort)) break;
