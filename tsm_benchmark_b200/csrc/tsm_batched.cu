@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -14,6 +15,7 @@
 #include "../../include/tsm.h"
 #include "tsm_errors.h"
 #include "tsm_batched.cuh"
+#include "tsm_tmap.h"
 
 namespace tsm {
 namespace {
@@ -24,7 +26,7 @@ constexpr uint32_t kMagic = 0x54534d42u;  // "TSMB"
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 struct Layout {
-  size_t problems, segments, cta_first, counters, partials, total;
+  size_t problems, maps, segments, cta_first, counters, partials, total;
 };
 
 Layout layout(int count, int nseg, int grid, size_t partial_doubles) {
@@ -32,6 +34,8 @@ Layout layout(int count, int nseg, int grid, size_t partial_doubles) {
   size_t off = kAlign;  // header: magic, error word
   l.problems = off;
   off = align_up(off + sizeof(BatchedProblemDev) * count);
+  l.maps = off;  // 2 tensor maps per problem (64-byte aligned: kAlign is 256)
+  off = align_up(off + sizeof(CUtensorMap) * 2 * count);
   l.segments = off;
   off = align_up(off + sizeof(BatchedSegmentDev) * nseg);
   l.cta_first = off;
@@ -77,6 +81,8 @@ tsm_status build_schedule(int count, const tsm_batched_problem_f64* in, int sms,
     const int cls = batched::class_of(q.m, q.k);
     if (cls < 0) return TSM_ERROR_UNSUPPORTED;  // widths outside {4, 8, 16, 32}
     if (q.n > 0 && (!aligned16(q.A) || !aligned16(q.B))) return TSM_ERROR_UNSUPPORTED;
+    // Tensor-core classes address rows with 32-bit tensor-map coordinates.
+    if (batched::dmma_class(q.m, q.k) && q.n > static_cast<int64_t>(INT_MAX) - 256) return TSM_ERROR_UNSUPPORTED;
     BatchedProblemDev& d = s.problems[p];
     d.A = q.A;
     d.B = q.B;
@@ -191,6 +197,22 @@ tsm_status tsm_batched_plan_init_f64(tsm_stream_t stream, int count, const tsm_b
   std::memcpy(img.data() + l.problems, s.problems.data(), sizeof(BatchedProblemDev) * count);
   std::memcpy(img.data() + l.segments, s.segments.data(), sizeof(BatchedSegmentDev) * nseg);
   std::memcpy(img.data() + l.cta_first, s.cta_first.data(), sizeof(int) * (s.grid + 1));
+  // Tensor maps of the tensor-core classes: 16-column x rows_of(m, k)-row
+  // boxes with the 128-byte swizzle the kernel reads with.
+  // (Encoded into an aligned local, then copied: the image's bytes carry no
+  // 64-byte alignment on the host.)
+  for (int p = 0; p < count; ++p) {
+    const BatchedProblemDev& d = s.problems[p];
+    if (!batched::dmma_class(d.m, d.k) || d.n == 0) continue;
+    const int rs = batched::rows_of(d.m, d.k);
+    CUtensorMap mp[2];
+    if (!encode_rowmajor_map(&mp[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, d.A, d.n, d.m, d.m, 16, rs,
+                             CU_TENSOR_MAP_SWIZZLE_128B, &last_error()) ||
+        !encode_rowmajor_map(&mp[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, d.B, d.n, d.k, d.k, 16, rs,
+                             CU_TENSOR_MAP_SWIZZLE_128B, &last_error()))
+      return TSM_ERROR_CUDA;
+    std::memcpy(img.data() + l.maps + sizeof(CUtensorMap) * 2 * p, mp, sizeof(mp));
+  }
   cudaStream_t cs = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemcpyAsync(device_buffer, img.data(), img.size(), cudaMemcpyHostToDevice, cs);
   if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
@@ -215,6 +237,7 @@ tsm_status tsm_gemm_tn_batched_f64(tsm_stream_t stream, const tsm_batched_plan* 
   unsigned char* base = static_cast<unsigned char*>(plan->device);
   BatchedArgs a{};
   a.problems = reinterpret_cast<const BatchedProblemDev*>(base + l.problems);
+  a.maps = reinterpret_cast<const CUtensorMap*>(base + l.maps);
   a.segments = reinterpret_cast<const BatchedSegmentDev*>(base + l.segments);
   a.cta_first = reinterpret_cast<const int*>(base + l.cta_first);
   a.counters = reinterpret_cast<unsigned*>(base + l.counters);

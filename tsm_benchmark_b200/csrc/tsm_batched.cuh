@@ -11,16 +11,22 @@
 //     bulk-copy ring (as tsm_plain.cuh), without pausing between segments or
 //     problems;
 //   * the consumer warps switch, per segment, to the compile-time path of the
-//     problem's width class (m, k in {4, 8, 16, 32}) -- exact register
-//     tiles, 16-byte rotated shared-memory loads -- and at the segment's end
-//     reduce their tiles (warp shuffles, then a fixed-order sum over warps in
-//     a shared-memory buffer separate from the ring) into the segment's FP64
-//     partial;
+//     problem's width class (m, k in {4, 8, 16, 32}) and at the segment's end
+//     reduce their tiles (a fixed-order sum over warps in a shared-memory
+//     buffer separate from the ring) into the segment's FP64 partial.  Classes
+//     with a width below 16 use SIMT register tiles over 1-D bulk copies
+//     (16-byte rotated shared-memory loads); classes with m, k in {16, 32} use
+//     the FP64 tensor cores (mma.sync m8n8k4 f64) over 2-D tiled TMA loads
+//     with the 128-byte swizzle, through two tensor maps per problem kept in
+//     the plan, with the fragment choice of tsm_dmma.cuh (conflict-free
+//     16-byte loads); rows a box brings in beyond the segment are zeroed in
+//     the fragments;
 //   * a per-problem counter finds the last segment of a problem to finish;
 //     that CTA sums the problem's partials in segment order and writes C_p.
 // Results are deterministic for a given plan; there are no atomics on data.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -53,6 +59,7 @@ struct BatchedSegmentDev {
 
 struct BatchedArgs {
   const BatchedProblemDev* problems;
+  const CUtensorMap* maps;  // 2 per problem (A, B); set for the tensor-core classes
   const BatchedSegmentDev* segments;
   const int* cta_first;  // segments of CTA b: [cta_first[b], cta_first[b + 1])
   unsigned* counters;    // one per problem, zero between launches
@@ -67,18 +74,25 @@ constexpr int kCT = kCW * 32;
 constexpr int kThreads = kCT + 32;
 constexpr int kStages = 4;
 constexpr int kStageBytes = 32768;
-// Largest slots x m x k doubles over the classes: 8 x 16 x 32 (and 4 x 32 x 32).
-constexpr int kRedBytes = 32768;
+// Largest slots x m x k doubles over the classes: 8 warps x 32 x 32.
+constexpr int kRedBytes = 65536;
 constexpr size_t kBarOffset = size_t(kStages) * kStageBytes + kRedBytes;
-constexpr size_t kSmemBytes = kBarOffset + 2 * kStages * sizeof(uint64_t) + 16;
+// + 1024: the ring is aligned to 1024 bytes (the swizzle pattern's period).
+constexpr size_t kSmemBytes = kBarOffset + 2 * kStages * sizeof(uint64_t) + 16 + 1024;
+
+// Tensor-core classes: both widths 16 or 32.
+__host__ __device__ constexpr bool dmma_class(int m, int k) { return m >= 16 && k >= 16; }
 
 // 4 x 4 register tiles for every class: sixteen inlined class paths share
 // one register budget, which nine warps per CTA cap at 168 per thread (three
 // warps on one SM sub-partition); larger tiles would spill.
 __host__ __device__ constexpr int tile_of(int) { return 4; }
 
-// Rows per chunk for widths (m, k): ~32 KB stages, whole row-group passes.
+// Rows per chunk for widths (m, k): ~32 KB stages.  SIMT classes: whole
+// row-group passes.  Tensor-core classes: (m + k) / 16 boxes of 128-byte rows,
+// rows a multiple of 32 (4-row k-steps split evenly over the 8 warps).
 __host__ __device__ constexpr int rows_of(int m, int k) {
+  if (dmma_class(m, k)) return (kStageBytes / (128 * ((m + k) / 16))) / 32 * 32;
   const int nt = (m / tile_of(m)) * (k / tile_of(k));
   const int rg = kCT / nt;
   const int rows = kStageBytes / (8 * (m + k));
@@ -92,6 +106,42 @@ __host__ __device__ constexpr int class_of(int m, int k) {
 }
 
 __device__ __forceinline__ void consumer_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(kCT) : "memory"); }
+
+// The end of a segment, after every consumer warp wrote its slot of the
+// M x K sheets in `red`: the fixed-order sum over the SLOTS sheets into the
+// segment's partial, then, for the problem's last segment to finish, the sum
+// of the problem's partials in segment order into C.
+template <int M, int K, int SLOTS>
+__device__ __forceinline__ void finish_segment(const BatchedArgs& a, const BatchedSegmentDev& seg,
+                                               const BatchedProblemDev& pr, double* red, unsigned* s_flag, int t) {
+  static_assert(SLOTS * M * K * 8 <= kRedBytes, "reduction buffer too small for this class");
+  consumer_barrier();
+  double* part = a.partials + seg.partial_off;
+  for (int e = t; e < M * K; e += kCT) {
+    double sum = red[e];
+#pragma unroll
+    for (int q = 1; q < SLOTS; ++q) sum += red[q * M * K + e];
+    part[e] = sum;
+  }
+  __threadfence();
+  consumer_barrier();
+  if (t == 0) {
+    const unsigned prev = atomicAdd(a.counters + seg.problem, 1u);
+    *s_flag = (prev == static_cast<unsigned>(pr.nseg - 1)) ? 1u : 0u;
+  }
+  consumer_barrier();
+  if (*s_flag) {
+    __threadfence();
+    const double* base = a.partials + a.segments[pr.seg_first].partial_off;
+    for (int e = t; e < M * K; e += kCT) {
+      double sum = dev::ld_cg(base + e);
+      for (int q = 1; q < pr.nseg; ++q) sum += dev::ld_cg(base + q * M * K + e);
+      double* c = pr.C + (e / K) * pr.ldc + (e % K);
+      *c = pr.accumulate ? *c + sum : sum;
+    }
+    if (t == 0) a.counters[seg.problem] = 0u;
+  }
+}
 
 // Consumes one segment of a (M, K) problem: its chunks from the ring, then
 // the CTA reduction into the segment's partial and, for the problem's last
@@ -167,39 +217,90 @@ __device__ __forceinline__ void consume_segment(const BatchedArgs& a, const Batc
 #pragma unroll
       for (int j = 0; j < TB; ++j) dst[(colA + i) * K + colB + j] = acc[i][j];
   }
-  consumer_barrier();
-  double* part = a.partials + seg.partial_off;
-  for (int e = t; e < M * K; e += kCT) {
-    double sum = red[e];
+  finish_segment<M, K, SLOTS>(a, seg, pr, red, s_flag, t);
+}
+
+// Consumes one segment of a tensor-core class (M, K in {16, 32}): every warp
+// holds all (M/8) x (K/8) 8x8 tiles of C and takes every 8th k-step (4 rows)
+// of each chunk; rows at or past the segment's end read as zero.
+template <int M, int K>
+__device__ __forceinline__ void consume_segment_dmma(const BatchedArgs& a, const BatchedSegmentDev& seg,
+                                                     const BatchedProblemDev& pr, unsigned char* ring, double* red,
+                                                     uint64_t* full, uint64_t* empty, volatile int* abort,
+                                                     unsigned* s_flag, int64_t& it, int t) {
+  constexpr int MT = M / 8, NT = K / 8;  // tiles along m and k
+  constexpr int MBA = M / 16;            // 16-column blocks of A (B's follow)
+  constexpr int RS = rows_of(M, K);
+  constexpr int BOX = RS * 128;
+  constexpr int KSTEPS = RS / 4;
+  static_assert(KSTEPS % kCW == 0, "k-steps must split evenly over the warps");
+  static_assert((M / 16 + K / 16) * BOX <= kStageBytes, "stage too small for this class");
+  const int warp = t >> 5, lane = t & 31;
+  const int g = lane >> 2, tq = lane & 3;
+  double acc[MT][NT][2];
 #pragma unroll
-    for (int q = 1; q < SLOTS; ++q) sum += red[q * M * K + e];
-    part[e] = sum;
-  }
-  __threadfence();
-  consumer_barrier();
-  if (t == 0) {
-    const unsigned prev = atomicAdd(a.counters + seg.problem, 1u);
-    *s_flag = (prev == static_cast<unsigned>(pr.nseg - 1)) ? 1u : 0u;
-  }
-  consumer_barrier();
-  if (*s_flag) {
-    __threadfence();
-    const double* base = a.partials + a.segments[pr.seg_first].partial_off;
-    for (int e = t; e < M * K; e += kCT) {
-      double sum = dev::ld_cg(base + e);
-      for (int q = 1; q < pr.nseg; ++q) sum += dev::ld_cg(base + q * M * K + e);
-      double* c = pr.C + (e / K) * pr.ldc + (e % K);
-      *c = pr.accumulate ? *c + sum : sum;
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  for (int64_t r0 = seg.r0; r0 < seg.r1; r0 += RS, ++it) {
+    const int s = static_cast<int>(it % kStages);
+    if (!*abort && !dev::mbar_wait(&full[s], static_cast<uint32_t>((it / kStages) & 1), abort)) {
+      *abort = 1;
+      atomicOr(a.error, dev::kErrTimeout);
     }
-    if (t == 0) a.counters[seg.problem] = 0u;
+    if (!*abort) {
+      const int rows = static_cast<int>((seg.r1 - r0) < RS ? (seg.r1 - r0) : RS);
+      const unsigned char* stage = ring + s * kStageBytes;
+#pragma unroll 2
+      for (int ks = warp; ks < KSTEPS; ks += kCW) {
+        const int row = 8 * (ks >> 1) + (ks & 1) + 2 * tq;
+        if (8 * (ks >> 1) + (ks & 1) >= rows) break;  // the k-step's first row is past the segment (warp-uniform)
+        const int off = row * 128 + ((g ^ (row & 7)) << 4);
+        const bool live = row < rows;
+        double av[MT], bv[NT];
+#pragma unroll
+        for (int i = 0; i < MT / 2; ++i) {
+          const double2 v = *reinterpret_cast<const double2*>(stage + i * BOX + off);
+          av[2 * i] = live ? v.x : 0.0;
+          av[2 * i + 1] = live ? v.y : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < NT / 2; ++j) {
+          const double2 v = *reinterpret_cast<const double2*>(stage + (MBA + j) * BOX + off);
+          bv[2 * j] = v.x;
+          bv[2 * j + 1] = v.y;
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) dev::dmma_m8n8k4(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) dev::mbar_arrive(&empty[s]);
   }
+
+  consumer_barrier();  // the previous segment's readers of `red` are done
+  // Tile (i, j): C row 16 (i / 2) + 2 g + (i & 1), column 16 (j / 2) + 2 (2 tq + e) + (j & 1).
+  double* dst = red + warp * M * K;
+#pragma unroll
+  for (int i = 0; i < MT; ++i) {
+    const int row = 16 * (i >> 1) + 2 * g + (i & 1);
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) dst[row * K + 16 * (j >> 1) + 2 * (2 * tq + e) + (j & 1)] = acc[i][j][e];
+  }
+  finish_segment<M, K, kCW>(a, seg, pr, red, s_flag, t);
 }
 
 }  // namespace batched
 
 __global__ void __launch_bounds__(batched::kThreads, 1) tsm_tn_batched_kernel(const BatchedArgs a) {
   using namespace batched;
-  extern __shared__ __align__(128) unsigned char smem[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((1024u - (dev::smem_u32(smem_raw) & 1023u)) & 1023u);
   unsigned char* ring = smem;
   double* red = reinterpret_cast<double*>(smem + size_t(kStages) * kStageBytes);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kBarOffset);
@@ -229,12 +330,28 @@ __global__ void __launch_bounds__(batched::kThreads, 1) tsm_tn_batched_kernel(co
       const BatchedSegmentDev seg = a.segments[si];
       const BatchedProblemDev& pr = a.problems[seg.problem];
       const int rs = rows_of(pr.m, pr.k);
+      const bool tc = dmma_class(pr.m, pr.k);
+      const CUtensorMap* ta = a.maps + 2 * seg.problem;
+      if (tc && lane == 0 && seg.r1 > seg.r0) {
+        dev::fence_tensormap_acquire(ta);
+        dev::fence_tensormap_acquire(ta + 1);
+      }
       for (int64_t r0 = seg.r0; r0 < seg.r1 && ok; r0 += rs, ++issued) {
         const int s = static_cast<int>(issued % kStages);
         const int64_t round = issued / kStages;
         if (lane == 0) {
           if (round > 0) ok = dev::mbar_wait(&empty[s], static_cast<uint32_t>((round - 1) & 1), abort);
-          if (ok) {
+          if (ok && tc) {
+            // Full 16-column x rs-row boxes (rows past n zero-filled; rows
+            // past the segment are masked by the consumers).
+            const int mba = pr.m / 16, mbb = pr.k / 16;
+            const int box = rs * 128;
+            unsigned char* st = ring + s * kStageBytes;
+            const int y = static_cast<int>(r0);
+            dev::mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>((mba + mbb) * box));
+            for (int b = 0; b < mba; ++b) dev::tma_load_2d(st + b * box, ta, 16 * b, y, &full[s], policy);
+            for (int b = 0; b < mbb; ++b) dev::tma_load_2d(st + (mba + b) * box, ta + 1, 16 * b, y, &full[s], policy);
+          } else if (ok) {
             const int64_t rows = (seg.r1 - r0) < rs ? (seg.r1 - r0) : rs;
             const uint32_t ba = static_cast<uint32_t>(rows * pr.m * sizeof(double));
             const uint32_t bb = static_cast<uint32_t>(rows * pr.k * sizeof(double));
@@ -261,14 +378,19 @@ __global__ void __launch_bounds__(batched::kThreads, 1) tsm_tn_batched_kernel(co
   case class_of(M, K):                                                                                  \
     consume_segment<M, K>(a, seg, pr, ring, red, full, empty, abort, s_flag, it, t);                    \
     break;
+#define TSM_BATCHED_TC_CASE(M, K)                                                                       \
+  case class_of(M, K):                                                                                  \
+    consume_segment_dmma<M, K>(a, seg, pr, ring, red, full, empty, abort, s_flag, it, t);               \
+    break;
       switch (pr.cls) {
         TSM_BATCHED_CASE(4, 4) TSM_BATCHED_CASE(4, 8) TSM_BATCHED_CASE(4, 16) TSM_BATCHED_CASE(4, 32)
         TSM_BATCHED_CASE(8, 4) TSM_BATCHED_CASE(8, 8) TSM_BATCHED_CASE(8, 16) TSM_BATCHED_CASE(8, 32)
-        TSM_BATCHED_CASE(16, 4) TSM_BATCHED_CASE(16, 8) TSM_BATCHED_CASE(16, 16) TSM_BATCHED_CASE(16, 32)
-        TSM_BATCHED_CASE(32, 4) TSM_BATCHED_CASE(32, 8) TSM_BATCHED_CASE(32, 16) TSM_BATCHED_CASE(32, 32)
+        TSM_BATCHED_CASE(16, 4) TSM_BATCHED_CASE(16, 8) TSM_BATCHED_TC_CASE(16, 16) TSM_BATCHED_TC_CASE(16, 32)
+        TSM_BATCHED_CASE(32, 4) TSM_BATCHED_CASE(32, 8) TSM_BATCHED_TC_CASE(32, 16) TSM_BATCHED_TC_CASE(32, 32)
         default:
           break;
       }
+#undef TSM_BATCHED_TC_CASE
 #undef TSM_BATCHED_CASE
     }
   }
