@@ -205,7 +205,7 @@ def tsmttsm_backward(A: torch.Tensor, B: torch.Tensor, dC: torch.Tensor, *, need
 def tsmttsm_split(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, accumulate: bool = False,
                   stream: torch.cuda.Stream | None = None) -> torch.Tensor:
     """C (float64) = A^T B for float32 A, B (m, k <= 32) on the tensor cores:
-    TF32 hi/lo split, FP32 accumulation per 64 rows, FP64 sums
+    TF32 hi/lo split, FP32 accumulation per 128 rows, FP64 sums
     (``tsm_gemm_tn_f32_split``)."""
     _check_operand(A, "A", torch.float32)
     _check_operand(B, "B", torch.float32)
