@@ -129,6 +129,7 @@ typedef struct tsm_variant_info {
   int exact;   /* 1: only m == wa, k == wb */
   int threads, stages, rows, unroll;
   size_t smem_bytes;
+  int gram;    /* 1: for C = A^T A only (B is A): streams A once, writes C symmetric */
 } tsm_variant_info;
 
 /* Number of compiled variants, and the description of one. */
@@ -139,6 +140,16 @@ tsm_status tsm_variant_get_info(int index, tsm_variant_info* info);
  * `stream`).  *bits != 0 means a kernel gave up a bounded wait and its C is
  * not valid; the call then returns TSM_ERROR_DEVICE_TIMEOUT. */
 tsm_status tsm_workspace_check(tsm_stream_t stream, void* workspace, unsigned* bits);
+
+/* C = A^T A (accumulate = 0) or C += A^T A, FP64: the Gram matrix of a tall
+ * and skinny A (n x m, pitch lda).  Reads A once -- half the bytes of
+ * tsm_gemm_tn_f64 on two operands -- and writes C exactly symmetric (each
+ * upper-triangle sum is written to both (i, j) and (j, i)).  tsm_gemm_tn_f64
+ * takes the same path when B is A (same pointer, pitch and width).  No
+ * counterpart in the reference (its drivers always pass distinct A and B,
+ * main.cc:63-64).  Workspace: tsm_gemm_tn_workspace_size(n, m, m). */
+tsm_status tsm_gram_f64(tsm_stream_t stream, int64_t n, int m, const double* A, int64_t lda, double* C, int64_t ldc,
+                        int accumulate, void* workspace, size_t workspace_bytes);
 
 /* C = A^T B (accumulate = 0) or C += A^T B (accumulate = 1), FP64, WITHOUT a
  * workspace.  No counterpart in the reference (its SYCL kernels need no

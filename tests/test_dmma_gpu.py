@@ -12,8 +12,9 @@ pytestmark = pytest.mark.gpu
 
 
 def dmma_variants():
+    """The two-operand DMMA variants (the Gram ones are in test_gram_gpu.py)."""
     from tsm_benchmark_b200 import variants
-    return [v for v in variants() if v["kind"] == "dmma"]
+    return [v for v in variants() if v["kind"] == "dmma" and not v["gram"]]
 
 
 def test_sixteen_dmma_variants_exist(gpu):

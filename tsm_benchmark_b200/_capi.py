@@ -52,6 +52,7 @@ class VariantInfo(ctypes.Structure):
         ("exact", c_int),
         ("threads", c_int), ("stages", c_int), ("rows", c_int), ("unroll", c_int),
         ("smem_bytes", c_size_t),
+        ("gram", c_int),
     ]
 
 
@@ -73,6 +74,8 @@ SIGNATURES = {
     "tsm_gemm_tn_workspace_size": (c_size_t, [c_int64, c_int, c_int]),
     "tsm_gemm_tn_f64": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                 c_void_p, c_int64, c_int, c_void_p, c_size_t]),
+    "tsm_gram_f64": (c_int, [c_void_p, c_int64, c_int, c_void_p, c_int64, c_void_p, c_int64, c_int, c_void_p,
+                             c_size_t]),
     "tsm_gemm_tn_f64_variant": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int, c_void_p, c_size_t, c_int]),
     "tsm_gemm_tn_f32": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
@@ -157,5 +160,5 @@ def variants() -> list[dict]:
                         dtype="f64" if info.dtype == 0 else "f32",
                         wa=info.wa, wb=info.wb, ta=info.ta, tb=info.tb, exact=bool(info.exact),
                         threads=info.threads, stages=info.stages, rows=info.rows, unroll=info.unroll,
-                        smem_bytes=info.smem_bytes))
+                        smem_bytes=info.smem_bytes, gram=bool(info.gram)))
     return out

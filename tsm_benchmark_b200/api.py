@@ -95,6 +95,34 @@ def tsmttsm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, 
     return C
 
 
+def gram(A: torch.Tensor, C: torch.Tensor | None = None, *, accumulate: bool = False,
+         stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """C = A^T A (or C += A^T A), FP64: reads A once and writes C exactly
+    symmetric (``tsm_gram_f64``).  ``tsmttsm(A, A)`` takes the same path.
+    Returns C; allocates it (m x m) when not given."""
+    _check_operand(A, "A", torch.float64)
+    n, m = A.shape
+    if C is None:
+        if accumulate:
+            raise ValueError("accumulate=True needs an existing C")
+        C = torch.empty((m, m), dtype=torch.float64, device=A.device)
+    else:
+        _check_operand(C, "C", torch.float64)
+        if tuple(C.shape) != (m, m):
+            raise ValueError(f"C must be {m}x{m}, got {tuple(C.shape)}")
+    lib = _capi.load()
+    with torch.cuda.device(A.device):
+        sh = _stream_handle(A.device, stream)
+        need = lib.tsm_gemm_tn_workspace_size(n, m, m)
+        if need == 0:
+            _capi.check(1, "tsm_gemm_tn_workspace_size")
+        ws = workspace(A.device, need, sh)
+        st = lib.tsm_gram_f64(sh, n, m, A.data_ptr(), _ld(A), C.data_ptr(), _ld(C), 1 if accumulate else 0,
+                              ws.data_ptr(), ws.numel())
+        _capi.check(st, "tsm_gram_f64")
+    return C
+
+
 def default_variant(A: torch.Tensor, B: torch.Tensor) -> int:
     """Index of the variant tsmttsm() would run for these operands."""
     lib = _capi.load()

@@ -42,13 +42,14 @@ def _cap(w: int) -> int:
 
 
 def candidates(variants: list[dict], m: int, k: int, dtype: str = "f64") -> list[dict]:
-    """Variants of `dtype` that accept (m, k): every exact one, and the
-    capacity ones no more than twice the smallest capacity per side (larger
-    ones only add masked work)."""
+    """Variants of `dtype` that accept (m, k) for distinct A and B: every
+    exact one, and the capacity ones no more than twice the smallest capacity
+    per side (larger ones only add masked work).  Gram variants (B is A)
+    are not candidates."""
     out = []
     cm, ck = _cap(m), _cap(k)
     for v in variants:
-        if v["dtype"] != dtype:
+        if v["dtype"] != dtype or v.get("gram"):
             continue
         if v["exact"]:
             if m == v["wa"] and k == v["wb"]:

@@ -68,6 +68,7 @@ class BulkVariant:
     unroll: int = 1
     exact: bool = True
     dtype: str = "f64"
+    gram: bool = False  # C = A^T A only: streams A once
 
     @property
     def esize(self) -> int:
@@ -82,7 +83,8 @@ class BulkVariant:
             return self
         rg = self.cw * 32 // self.num_tiles
         e = self.epc
-        rows = max(e, (32768 // (self.esize * (self.wa + self.wb))) // e * e)
+        width = self.wa if self.gram else self.wa + self.wb
+        rows = max(e, (32768 // (self.esize * width)) // e * e)
         # Round to whole passes of the row groups, keeping every bulk copy a
         # multiple of 16 bytes.
         if rows >= rg:
@@ -100,14 +102,15 @@ class BulkVariant:
         kind = "bulk" if v.dtype == "f64" else "bulkf32"
         s = (f"{kind}_{v.wa}x{v.wb}_t{v.ta}x{v.tb}_w{v.cw}_s{v.stages}"
              f"_r{v.rows}_u{v.unroll}")
-        return s if v.exact else s + "_cap"
+        s = s if v.exact else s + "_cap"
+        return s + "_gram" if v.gram else s
 
     def smem_bytes(self) -> int:
         v = self.resolved()
         ct = v.cw * 32
         nt = v.num_tiles
         slots = v.cw if nt < 32 else ct // nt
-        ring = v.stages * v.rows * (v.wa + v.wb) * v.esize
+        ring = v.stages * v.rows * (v.wa if v.gram else v.wa + v.wb) * v.esize
         red = slots * v.wa * v.wb * 8
         data = max(ring, red)
         return (data + 127) // 128 * 128 + 2 * v.stages * 8 + 16
@@ -131,6 +134,8 @@ class BulkVariant:
             errs.append("unroll must divide the rows per thread")
         if v.ta * v.tb > 64:
             errs.append("register tile above 64 accumulators")
+        if v.gram and not (v.exact and v.wa == v.wb):
+            errs.append("Gram variants are exact and square")
         if self.smem_bytes() > SMEM_LIMIT:
             errs.append(f"shared memory {self.smem_bytes()} above {SMEM_LIMIT}")
         return errs
@@ -140,7 +145,7 @@ class BulkVariant:
         ctype = "double" if v.dtype == "f64" else "float"
         return (f'TSM_BULK_VARIANT("{self.name}", {ctype}, {v.wa}, {v.wb}, {v.ta}, {v.tb}, '
                 f'{v.cw}, {v.stages}, {v.rows}, {v.unroll}, '
-                f'{"true" if v.exact else "false"})')
+                f'{"true" if v.exact else "false"}, {"true" if v.gram else "false"})')
 
 
 @dataclasses.dataclass(frozen=True)
@@ -198,6 +203,7 @@ class DmmaVariant:
     rows: int = 0    # 0: ~64 KB stages
     dtype: str = "f64"
     exact: bool = True
+    gram: bool = False  # C = A^T A only: streams A once
 
     @staticmethod
     def best_region(wa: int, wb: int) -> tuple[int, int]:
@@ -216,18 +222,20 @@ class DmmaVariant:
 
     @property
     def regions(self) -> int:
+        if self.gram:  # upper-triangle block-pair regions of tsm_gram_dmma_kernel
+            return {16: 1, 32: 1, 48: 2, 64: 3}[self.wa]
         mt, nt = (self.mt, self.nt) if self.mt else self.best_region(self.wa, self.wb)
         return ((self.wa // 8) // mt) * ((self.wb // 8) // nt)
 
     def resolved(self) -> "DmmaVariant":
         v = self
-        if not v.mt:
+        if not v.mt and not v.gram:
             mt, nt = self.best_region(v.wa, v.wb)
             v = dataclasses.replace(v, mt=mt, nt=nt)
         if not v.cw:
             r = v.regions
             v = dataclasses.replace(v, cw=r * max(1, -(-8 // r)))
-        blocks = v.wa // 16 + v.wb // 16
+        blocks = v.wa // 16 + (0 if v.gram else v.wb // 16)
         if not v.rows:
             # whole 8-row swizzle groups and an equal number of 4-row k-steps
             # for every row slot
@@ -242,12 +250,14 @@ class DmmaVariant:
     @property
     def name(self) -> str:
         v = self.resolved()
+        if v.gram:
+            return f"dmma_{v.wa}x{v.wb}_gram_w{v.cw}_s{v.stages}_r{v.rows}"
         return f"dmma_{v.wa}x{v.wb}_t{8 * v.mt}x{8 * v.nt}_w{v.cw}_s{v.stages}_r{v.rows}"
 
     def smem_bytes(self) -> int:
         v = self.resolved()
         slots = v.cw // v.regions
-        ring = v.stages * (v.wa // 16 + v.wb // 16) * v.rows * 128
+        ring = v.stages * (v.wa // 16 + (0 if v.gram else v.wb // 16)) * v.rows * 128
         red = slots * v.wa * v.wb * 8
         return 1024 + (max(ring, red) + 127) // 128 * 128 + 2 * v.stages * 8 + 16
 
@@ -256,7 +266,7 @@ class DmmaVariant:
         errs = []
         if v.wa % 16 or v.wb % 16 or not (16 <= v.wa <= 64 and 16 <= v.wb <= 64):
             errs.append("widths must be multiples of 16 in 16..64")
-        if v.mt % 2 or v.nt % 2 or (v.wa // 8) % v.mt or (v.wb // 8) % v.nt or v.mt * v.nt > 16:
+        if not v.gram and (v.mt % 2 or v.nt % 2 or (v.wa // 8) % v.mt or (v.wb // 8) % v.nt or v.mt * v.nt > 16):
             errs.append("region: even tile counts dividing the widths, at most 16 tiles")
         if v.cw % v.regions:
             errs.append("consumer warps must cover whole regions")
@@ -268,12 +278,16 @@ class DmmaVariant:
             errs.append("chunk k-steps must split evenly over the row slots")
         if v.dtype != "f64":
             errs.append("FP64 only")
+        if v.gram and v.wa != v.wb:
+            errs.append("Gram variants are square")
         if self.smem_bytes() > SMEM_LIMIT:
             errs.append(f"shared memory {self.smem_bytes()} above {SMEM_LIMIT}")
         return errs
 
     def emit(self) -> str:
         v = self.resolved()
+        if v.gram:
+            return f'TSM_GRAM_DMMA_VARIANT("{self.name}", {v.wa}, {v.cw}, {v.stages}, {v.rows})'
         return f'TSM_DMMA_VARIANT("{self.name}", {v.wa}, {v.wb}, {v.mt}, {v.nt}, {v.cw}, {v.stages}, {v.rows})'
 
 
@@ -332,6 +346,12 @@ def default_variants() -> list:
     for wa in WIDTH_CAPS:
         for wb in WIDTH_CAPS:
             out.append(DirectVariant(wa, wb, default_tile(wa), default_tile(wb), dtype="f32"))
+    # Gram C = A^T A (A streamed once), last so that earlier indices stay put:
+    # tensor cores for the DMMA widths, SIMT register tiles below 16.
+    for w in DMMA_WIDTHS:
+        out.append(DmmaVariant(w, w, gram=True))
+    for w in (1, 2, 4, 8):
+        out.append(BulkVariant(w, w, default_tile(w), default_tile(w), gram=True))
     return out
 
 
@@ -419,7 +439,7 @@ def compat_variant_for(vs: list, m: int, tm: int) -> str | None:
     """The exact bulk variant whose register tile is the reference's TM x TM
     for width m, else None (the library default is used)."""
     for v in vs:
-        if isinstance(v, BulkVariant) and v.exact and v.dtype == "f64" \
+        if isinstance(v, BulkVariant) and v.exact and v.dtype == "f64" and not v.gram \
                 and (v.wa, v.wb, v.ta, v.tb) == (m, m, tm, tm) and v.unroll == 1 and v.cw == 8 and v.stages == 6:
             return v.name
     return None

@@ -98,9 +98,15 @@ tsm_status prepare_variant(DeviceState* st, int idx) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// C = A^T A: B is the same matrix as A (same data, pitch and width).
+bool is_gram(int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
+  return A == B && lda == ldb && m == k;
+}
+
 bool applicable(const Variant* v, int dtype, int64_t n, int m, int k, const void* A, int64_t lda, const void* B,
                 int64_t ldb) {
   if (v->dtype != dtype) return false;
+  if (v->gram && !is_gram(m, k, A, lda, B, ldb)) return false;
   if (v->exact ? (m != v->wa || k != v->wb) : (m > v->wa || k > v->wb)) return false;
   if (v->kind == kKindBulk) {
     if (lda != m || ldb != k) return false;
@@ -144,6 +150,10 @@ int find_variant(const char* name) {
 
 int default_variant(int dtype, int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
   const auto& vs = variants();
+  // 0. C = A^T A: a Gram variant (A streamed once), in table order.
+  if (is_gram(m, k, A, lda, B, ldb))
+    for (size_t i = 0; i < vs.size(); ++i)
+      if (vs[i]->gram && applicable(vs[i], dtype, n, m, k, A, lda, B, ldb)) return static_cast<int>(i);
   // 1. The tuning table: the entry with the largest nmin <= n for (m, k).
   int best = -1;
   long long best_nmin = -1;
@@ -225,9 +235,10 @@ tsm_status launch_variant(const Variant* v, const PlainArgs<T>& p, int64_t grid,
     if constexpr (sizeof(T) == 8) {
       DmmaArgs d{};
       d.p = p;
+      d.p.symmetric = is_gram(p.m, p.k, p.A, p.lda, p.B, p.ldb) ? 1 : 0;
       if (p.n > 0) {  // n = 0: no chunks, the maps are never read
         tsm_status s = encode_operand_map(&d.ta, p.A, p.n, p.m, p.lda, v->rows);
-        if (s == TSM_SUCCESS) s = encode_operand_map(&d.tb, p.B, p.n, p.k, p.ldb, v->rows);
+        if (s == TSM_SUCCESS && !v->gram) s = encode_operand_map(&d.tb, p.B, p.n, p.k, p.ldb, v->rows);
         if (s != TSM_SUCCESS) return s;
       }
       void* args[] = {&d};
@@ -237,6 +248,7 @@ tsm_status launch_variant(const Variant* v, const PlainArgs<T>& p, int64_t grid,
     }
   } else {
     PlainArgs<T> q = p;
+    q.symmetric = is_gram(p.m, p.k, p.A, p.lda, p.B, p.ldb) ? 1 : 0;  // C = A^T A: written exactly symmetric
     void* args[] = {&q};
     e = cudaLaunchKernel(v->kernel, dim3(static_cast<unsigned>(grid)), dim3(v->threads), args, v->smem, stream);
   }
@@ -339,6 +351,12 @@ tsm_status tsm_gemm_tn_f64(tsm_stream_t stream, int64_t n, int m, int k, const d
                               workspace, workspace_bytes, -1);
 }
 
+tsm_status tsm_gram_f64(tsm_stream_t stream, int64_t n, int m, const double* A, int64_t lda, double* C, int64_t ldc,
+                        int accumulate, void* workspace, size_t workspace_bytes) {
+  return launch_plain<double>(static_cast<cudaStream_t>(stream), n, m, m, A, lda, A, lda, C, ldc, accumulate,
+                              workspace, workspace_bytes, -1);
+}
+
 tsm_status tsm_gemm_tn_f64_variant(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
                                    const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
                                    void* workspace, size_t workspace_bytes, int variant) {
@@ -386,6 +404,7 @@ tsm_status tsm_variant_get_info(int index, tsm_variant_info* info) {
   info->rows = v->rows;
   info->unroll = v->unroll;
   info->smem_bytes = v->smem;
+  info->gram = v->gram;
   return TSM_SUCCESS;
 }
 

@@ -218,3 +218,229 @@ __global__ void __launch_bounds__(DmmaTn<WA, WB, MT, NT, CW, STAGES, RS>::THREAD
 }
 
 }  // namespace tsm
+
+namespace tsm {
+
+// ---------------------------------------------------------------------------
+// Gram C = A^T A on the FP64 tensor cores, upper triangle only.
+//
+// The 16-column blocks b of A give 8x8 tiles 2b (even columns) and 2b + 1
+// (odd columns).  Only block pairs (bi, bj) with bi <= bj are computed -- 4
+// tiles each, the lower tile of a diagonal pair included -- so C's upper
+// triangle is complete and the lower one is written by mirroring
+// (finish_partials with symmetric = 1).  Per k-step a warp loads each 16-column
+// block its region touches ONCE and feeds both DMMA operands from it (B is A).
+// Regions (lists of block pairs, <= 16 tiles):
+//   W = 16: {(0,0)}                              1 region
+//   W = 32: {(0,0),(0,1),(1,1)}                  1 region, 12 of 16 tiles
+//   W = 48: {(0,0),(0,1),(1,1)}, {(0,2),(1,2),(2,2)}           24 of 36 tiles
+//   W = 64: {(0,0),(0,1),(1,1)}, {(2,2),(2,3),(3,3)},
+//           {(0,2),(0,3),(1,2),(1,3)}                          40 of 64 tiles
+// A pair is coded 4 bi + bj, four bits per pair.
+__host__ __device__ constexpr int gram_regions(int W) { return W == 64 ? 3 : (W == 48 ? 2 : 1); }
+__host__ __device__ constexpr int gram_npairs(int W, int r) {
+  return W == 16 ? 1 : (W == 64 && r == 2 ? 4 : 3);
+}
+__host__ __device__ constexpr unsigned gram_pair_codes(int W, int r) {
+  return W == 16 ? 0x0u
+         : r == 0 ? (0x0u | (0x1u << 4) | (0x5u << 8))
+         : (W == 48 || r == 2) ? (W == 48 ? (0x2u | (0x6u << 4) | (0xAu << 8))
+                                          : (0x2u | (0x3u << 4) | (0x6u << 8) | (0x7u << 12)))
+                               : (0xAu | (0xBu << 4) | (0xFu << 8));
+}
+__host__ __device__ constexpr int gram_pair(int W, int r, int p) {
+  return static_cast<int>((gram_pair_codes(W, r) >> (4 * p)) & 0xFu);
+}
+// Blocks a region touches (bit b: 16-column block b).
+__host__ __device__ constexpr unsigned gram_block_mask(int W, int r) {
+  unsigned mask = 0;
+  for (int p = 0; p < gram_npairs(W, r); ++p) mask |= (1u << (gram_pair(W, r, p) >> 2)) | (1u << (gram_pair(W, r, p) & 3));
+  return mask;
+}
+
+template <int W, int CW, int STAGES, int RS>
+struct GramDmma {
+  static_assert(W % 16 == 0 && W >= 16 && W <= 64, "width: multiple of 16 up to 64");
+  static_assert(RS % 8 == 0 && RS <= 256, "chunk rows: whole 8-row swizzle groups, TMA box <= 256");
+  static constexpr int NB = W / 16;
+  static constexpr int R = gram_regions(W);
+  static_assert(CW % R == 0, "consumer warps must cover whole regions");
+  static constexpr int S = CW / R;
+  static constexpr int KSTEPS = RS / 4;
+  static constexpr int BOX_BYTES = RS * 128;
+  static constexpr int STAGE_BYTES = NB * BOX_BYTES;
+  static constexpr int THREADS = CW * 32 + 32;
+  static constexpr size_t RING_BYTES = size_t(STAGES) * STAGE_BYTES;
+  static constexpr size_t RED_BYTES = size_t(S) * W * W * sizeof(double);
+  static constexpr size_t DATA_BYTES = RING_BYTES > RED_BYTES ? RING_BYTES : RED_BYTES;
+  static constexpr size_t BAR_OFFSET = (DATA_BYTES + 127) / 128 * 128;
+  static constexpr size_t SMEM_BYTES = 1024 + BAR_OFFSET + 2 * STAGES * sizeof(uint64_t) + 16;
+};
+
+namespace detail {
+
+// One consumer warp of region REG: every chunk's k-steps of its slot, then
+// its tiles into the slot's sheet of `red` (after the caller's barrier).
+template <int W, int CW, int STAGES, int RS, int REG>
+__device__ __forceinline__ void gram_consume(const PlainArgs<double>& p, unsigned char* smem, uint64_t* full,
+                                             uint64_t* empty, volatile int* abort, int slot, int lane,
+                                             double (&out)[4][2][2][2]) {
+  using K = GramDmma<W, CW, STAGES, RS>;
+  constexpr int NP = gram_npairs(W, REG);
+  constexpr unsigned MASK = gram_block_mask(W, REG);
+  const int g = lane >> 2, tq = lane & 3;
+  const int64_t G = gridDim.x;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) out[q][a][b][0] = out[q][a][b][1] = 0.0;
+  int64_t it = 0;
+  for (int64_t c = blockIdx.x; c < p.num_chunks; c += G, ++it) {
+    const int s = static_cast<int>(it % STAGES);
+    if (!dev::mbar_wait(&full[s], static_cast<uint32_t>((it / STAGES) & 1), abort)) {
+      *abort = 1;
+      atomicOr(p.error, dev::kErrTimeout);
+      break;
+    }
+    const unsigned char* stage = smem + s * K::STAGE_BYTES;
+#pragma unroll 2
+    for (int ks = slot; ks < K::KSTEPS; ks += K::S) {
+      const int row = 8 * (ks >> 1) + (ks & 1) + 2 * tq;
+      const int off = row * 128 + ((g ^ (row & 7)) << 4);
+      double v[K::NB][2];
+#pragma unroll
+      for (int b = 0; b < K::NB; ++b) {
+        if (MASK & (1u << b)) {
+          const double2 x = *reinterpret_cast<const double2*>(stage + b * K::BOX_BYTES + off);
+          v[b][0] = x.x;
+          v[b][1] = x.y;
+        } else {
+          v[b][0] = v[b][1] = 0.0;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        const int bi = gram_pair(W, REG, q) >> 2, bj = gram_pair(W, REG, q) & 3;
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b) dev::dmma_m8n8k4(out[q][a][b][0], out[q][a][b][1], v[bi][a], v[bj][b]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) dev::mbar_arrive(&empty[s]);
+  }
+}
+
+// Tile (pair q, parities a, b) -> C row 16 bi + 2 g + a, column 16 bj + 2 n + b
+// for D column n = 2 tq + e.
+template <int W, int REG>
+__device__ __forceinline__ void gram_store(double* sheet, int lane, const double (&out)[4][2][2][2]) {
+  constexpr int NP = gram_npairs(W, REG);
+  const int g = lane >> 2, tq = lane & 3;
+#pragma unroll
+  for (int q = 0; q < NP; ++q) {
+    const int bi = gram_pair(W, REG, q) >> 2, bj = gram_pair(W, REG, q) & 3;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          sheet[(16 * bi + 2 * g + a) * W + 16 * bj + 2 * (2 * tq + e) + b] = out[q][a][b][e];
+  }
+}
+
+}  // namespace detail
+
+template <int W, int CW, int STAGES, int RS>
+__global__ void __launch_bounds__(GramDmma<W, CW, STAGES, RS>::THREADS, 1)
+    tsm_gram_dmma_kernel(const __grid_constant__ DmmaArgs args) {
+  using K = GramDmma<W, CW, STAGES, RS>;
+  const PlainArgs<double>& p = args.p;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((1024u - (dev::smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + K::BAR_OFFSET);
+  uint64_t* empty = full + STAGES;
+  volatile int* abort = reinterpret_cast<volatile int*>(empty + STAGES);
+  unsigned* s_is_last = reinterpret_cast<unsigned*>(empty + STAGES) + 1;
+
+  const int t = threadIdx.x;
+  const int warp = t >> 5, lane = t & 31;
+  if (t == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      dev::mbar_init(&full[s], 1);
+      dev::mbar_init(&empty[s], CW);
+    }
+    *abort = 0;
+    dev::fence_mbar_init();
+  }
+  if (warp == CW && lane == 0 && blockIdx.x < p.num_chunks) dev::prefetch_tensormap(&args.ta);
+  __syncthreads();
+
+  const int64_t G = gridDim.x;
+  const int region = warp % K::R, slot = warp / K::R;
+  double out[4][2][2][2];
+
+  if (warp == CW) {
+    // ---------------- producer warp: A's boxes only.
+    int64_t issued = 0;
+    const uint64_t policy = dev::policy_evict_first();
+    for (int64_t c = blockIdx.x; c < p.num_chunks; c += G, ++issued) {
+      const int s = static_cast<int>(issued % STAGES);
+      const int64_t round = issued / STAGES;
+      bool ok = true;
+      if (lane == 0) {
+        if (round > 0) ok = dev::mbar_wait(&empty[s], static_cast<uint32_t>((round - 1) & 1), abort);
+        if (ok) {
+          unsigned char* stage = smem + s * K::STAGE_BYTES;
+          const int y = static_cast<int>(c * RS);
+          dev::mbar_arrive_expect_tx(&full[s], K::STAGE_BYTES);
+#pragma unroll
+          for (int b = 0; b < K::NB; ++b)
+            dev::tma_load_2d(stage + b * K::BOX_BYTES, &args.ta, 16 * b, y, &full[s], policy);
+        } else {
+          *abort = 1;
+          atomicOr(p.error, dev::kErrTimeout);
+        }
+      }
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) break;
+    }
+  } else if (region == 0) {
+    detail::gram_consume<W, CW, STAGES, RS, 0>(p, smem, full, empty, abort, slot, lane, out);
+  } else if (region == 1) {
+    detail::gram_consume<W, CW, STAGES, RS, (K::R > 1 ? 1 : 0)>(p, smem, full, empty, abort, slot, lane, out);
+  } else {
+    detail::gram_consume<W, CW, STAGES, RS, (K::R > 2 ? 2 : 0)>(p, smem, full, empty, abort, slot, lane, out);
+  }
+
+  __syncthreads();
+  if (*abort && warp == CW && lane == 0) {
+    int64_t issued = 0;
+    for (int64_t c = blockIdx.x; c < p.num_chunks; c += G) ++issued;
+    volatile int no_abort = 0;
+    for (int64_t q = issued > STAGES ? issued - STAGES : 0; q < issued; ++q)
+      if (!dev::mbar_wait(&full[q % STAGES], static_cast<uint32_t>((q / STAGES) & 1), &no_abort)) break;
+  }
+  __syncthreads();
+
+  // Tiles -> the slot's W x W sheet (the upper triangle is complete; cells
+  // below the diagonal blocks are never read by the symmetric finish).
+  double* red = reinterpret_cast<double*>(smem);
+  if (warp < CW) {
+    double* sheet = red + slot * (W * W);
+    if (region == 0)
+      detail::gram_store<W, 0>(sheet, lane, out);
+    else if (region == 1)
+      detail::gram_store<W, (K::R > 1 ? 1 : 0)>(sheet, lane, out);
+    else
+      detail::gram_store<W, (K::R > 2 ? 2 : 0)>(sheet, lane, out);
+  }
+  __syncthreads();
+  detail::finish_partials(p, red, K::S, t, K::THREADS, s_is_last);
+}
+
+}  // namespace tsm

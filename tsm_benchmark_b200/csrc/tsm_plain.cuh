@@ -42,6 +42,7 @@ struct PlainArgs {
   int k;      // columns of B = columns of C
   int64_t lda, ldb, ldc;
   int accumulate;      // 1: C += A^T B (the reference's semantics), 0: C = A^T B
+  int symmetric;       // 1: B is A (m == k): C = A^T A is written from its upper triangle, mirrored
   int64_t rows_main;   // rows covered by the main loop; rows [rows_main, n) are added at the end
   int64_t num_chunks;  // bulk kernel: ceil(rows_main / RS)
   double* partials;    // workspace: gridDim.x * m * k doubles
@@ -218,16 +219,23 @@ __device__ __forceinline__ void finish_partials(const PlainArgs<T>& p, const dou
   if (*s_is_last == 0u) return;
 
   // 4. Last CTA: partials in CTA order, then the leftover rows, then C.
+  //    Symmetric (Gram): the upper triangle is summed and written to both
+  //    (i, j) and (j, i), so C is exactly symmetric.
   __threadfence();
   const int G = gridDim.x;
   for (int e = t; e < mk; e += nthreads) {
     const int i = e / k, j = e - (e / k) * k;
+    if (p.symmetric && i > j) continue;
     double s = dev::ld_cg(p.partials + e);
     for (int b = 1; b < G; ++b) s += dev::ld_cg(p.partials + static_cast<int64_t>(b) * mk + e);
     for (int64_t r = p.rows_main; r < p.n; ++r)
       s += static_cast<double>(p.A[r * p.lda + i]) * static_cast<double>(p.B[r * p.ldb + j]);
     T* c = p.C + static_cast<int64_t>(i) * p.ldc + j;
     *c = static_cast<T>(p.accumulate ? static_cast<double>(*c) + s : s);
+    if (p.symmetric && i != j) {
+      T* ct = p.C + static_cast<int64_t>(j) * p.ldc + i;
+      *ct = static_cast<T>(p.accumulate ? static_cast<double>(*ct) + s : s);
+    }
   }
   if (t == 0) *p.counter = 0u;  // ready for the next launch on this workspace
 }
@@ -272,8 +280,12 @@ __device__ __forceinline__ void load_row_seg(T (&v)[W], const T* src, int valid,
 // --------------------------------------------------------------------------
 // Bulk (TMA) pipelined kernel.
 // --------------------------------------------------------------------------
-template <typename T, int WA, int WB, int TA, int TB, int CW, int STAGES, int RS, int UNROLL, bool EXACT>
+// GRAM: B is A (C = A^T A): only A's rows are streamed and the B tile reads
+// the same stage.
+template <typename T, int WA, int WB, int TA, int TB, int CW, int STAGES, int RS, int UNROLL, bool EXACT,
+          bool GRAM = false>
 struct BulkKernel {
+  static_assert(!GRAM || (WA == WB && EXACT), "Gram variants are exact and square");
   using S = TileShape<WA, WB, TA, TB>;
   static constexpr int EPC = 16 / int(sizeof(T));  // elements per 16-byte chunk
   static constexpr int CT = CW * 32;               // consumer threads
@@ -282,7 +294,7 @@ struct BulkKernel {
   static constexpr int RG = CT / S::NT;  // row groups
   static_assert(RS % EPC == 0, "chunk rows must keep every bulk copy a multiple of 16 bytes");
   static constexpr int STAGE_A = RS * WA;  // elements (capacity)
-  static constexpr int STAGE_B = RS * WB;
+  static constexpr int STAGE_B = GRAM ? 0 : RS * WB;
   static constexpr int SLOTS = S::NT < 32 ? CW : RG;
   static constexpr size_t RING_BYTES = size_t(STAGES) * (STAGE_A + STAGE_B) * sizeof(T);
   static constexpr size_t RED_BYTES = size_t(SLOTS) * WA * WB * sizeof(double);
@@ -306,10 +318,11 @@ struct BulkKernel {
   }
 };
 
-template <typename T, int WA, int WB, int TA, int TB, int CW, int STAGES, int RS, int UNROLL, bool EXACT>
-__global__ void __launch_bounds__(BulkKernel<T, WA, WB, TA, TB, CW, STAGES, RS, UNROLL, EXACT>::THREADS, 1)
+template <typename T, int WA, int WB, int TA, int TB, int CW, int STAGES, int RS, int UNROLL, bool EXACT,
+          bool GRAM = false>
+__global__ void __launch_bounds__(BulkKernel<T, WA, WB, TA, TB, CW, STAGES, RS, UNROLL, EXACT, GRAM>::THREADS, 1)
     tsm_tn_bulk_kernel(const PlainArgs<T> p) {
-  using K = BulkKernel<T, WA, WB, TA, TB, CW, STAGES, RS, UNROLL, EXACT>;
+  using K = BulkKernel<T, WA, WB, TA, TB, CW, STAGES, RS, UNROLL, EXACT, GRAM>;
   using S = typename K::S;
   extern __shared__ __align__(128) unsigned char smem[];
   T* ringA = reinterpret_cast<T*>(smem);
@@ -355,10 +368,10 @@ __global__ void __launch_bounds__(BulkKernel<T, WA, WB, TA, TB, CW, STAGES, RS, 
           const int64_t r0 = c * RS;
           const int64_t rows = (p.rows_main - r0) < RS ? (p.rows_main - r0) : RS;
           const uint32_t ba = static_cast<uint32_t>(rows * m * sizeof(T));
-          const uint32_t bb = static_cast<uint32_t>(rows * k * sizeof(T));
+          const uint32_t bb = GRAM ? 0u : static_cast<uint32_t>(rows * k * sizeof(T));
           dev::mbar_arrive_expect_tx(&full[s], ba + bb);
           dev::bulk_g2s_evict_first(ringA + s * K::STAGE_A, p.A + r0 * m, ba, &full[s], policy);
-          dev::bulk_g2s_evict_first(ringB + s * K::STAGE_B, p.B + r0 * k, bb, &full[s], policy);
+          if (!GRAM) dev::bulk_g2s_evict_first(ringB + s * K::STAGE_B, p.B + r0 * k, bb, &full[s], policy);
         } else {
           *abort = 1;
           atomicOr(p.error, dev::kErrTimeout);
@@ -387,7 +400,7 @@ __global__ void __launch_bounds__(BulkKernel<T, WA, WB, TA, TB, CW, STAGES, RS, 
       const int64_t r0 = c * RS;
       const int rows = static_cast<int>((p.rows_main - r0) < RS ? (p.rows_main - r0) : RS);
       const T* sa = ringA + s * K::STAGE_A + colA;
-      const T* sb = ringB + s * K::STAGE_B + colB;
+      const T* sb = (GRAM ? ringA + s * K::STAGE_A : ringB + s * K::STAGE_B) + colB;
       if (rows == RS) {
         static_assert((RS / K::RG) % UNROLL == 0 || RS < K::RG, "unroll must divide the rows per thread");
 #pragma unroll UNROLL

@@ -42,6 +42,7 @@ struct Variant {
   int unroll;   // bulk: row-loop unroll
   size_t smem;  // dynamic shared memory per CTA
   const void* kernel;
+  int gram;     // 1: B must be A (m == k, same data): streams A once, C written symmetric
 };
 
 struct VariantPart {
@@ -55,25 +56,34 @@ extern const int kVariantPartCount;
 
 }  // namespace tsm
 
-#define TSM_BULK_VARIANT(NAME, T, WA, WB, TA, TB, CW, ST, RS, U, EX)                                     \
+#define TSM_BULK_VARIANT(NAME, T, WA, WB, TA, TB, CW, ST, RS, U, EX, GR)                                 \
   ::tsm::Variant {                                                                                       \
     NAME, ::tsm::kKindBulk, ::tsm::DTypeOf<T>::value, WA, WB, TA, TB, EX,                                \
-        ::tsm::BulkKernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX>::THREADS, ST, RS, U,                     \
-        ::tsm::BulkKernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX>::SMEM_BYTES,                             \
-        reinterpret_cast<const void*>(&::tsm::tsm_tn_bulk_kernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX>)  \
+        ::tsm::BulkKernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX, GR>::THREADS, ST, RS, U,                 \
+        ::tsm::BulkKernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX, GR>::SMEM_BYTES,                         \
+        reinterpret_cast<const void*>(&::tsm::tsm_tn_bulk_kernel<T, WA, WB, TA, TB, CW, ST, RS, U, EX, GR>), GR \
   }
 
 #define TSM_DIRECT_VARIANT(NAME, T, WA, WB, TA, TB, TH, EX)                                        \
   ::tsm::Variant {                                                                                 \
     NAME, ::tsm::kKindDirect, ::tsm::DTypeOf<T>::value, WA, WB, TA, TB, EX, TH, 0, 0, 1,           \
         ::tsm::DirectKernel<T, WA, WB, TA, TB, TH, EX>::SMEM_BYTES,                                \
-        reinterpret_cast<const void*>(&::tsm::tsm_tn_direct_kernel<T, WA, WB, TA, TB, TH, EX>)     \
+        reinterpret_cast<const void*>(&::tsm::tsm_tn_direct_kernel<T, WA, WB, TA, TB, TH, EX>), 0  \
   }
 
-#define TSM_DMMA_VARIANT(NAME, WA, WB, MT, NT, CW, ST, RS)                                                 \
-  ::tsm::Variant {                                                                                         \
-    NAME, ::tsm::kKindDmma, ::tsm::kF64, WA, WB, MT * 8, NT * 8, 1,                                          \
-        ::tsm::DmmaTn<WA, WB, MT, NT, CW, ST, RS>::THREADS, ST, RS, 1,                                       \
-        ::tsm::DmmaTn<WA, WB, MT, NT, CW, ST, RS>::SMEM_BYTES,                                               \
-        reinterpret_cast<const void*>(&::tsm::tsm_tn_dmma_kernel<WA, WB, MT, NT, CW, ST, RS>)                \
+#define TSM_DMMA_VARIANT(NAME, WA, WB, MT, NT, CW, ST, RS)                                               \
+  ::tsm::Variant {                                                                                       \
+    NAME, ::tsm::kKindDmma, ::tsm::kF64, WA, WB, MT * 8, NT * 8, 1,                                        \
+        ::tsm::DmmaTn<WA, WB, MT, NT, CW, ST, RS>::THREADS, ST, RS, 1,                                     \
+        ::tsm::DmmaTn<WA, WB, MT, NT, CW, ST, RS>::SMEM_BYTES,                                             \
+        reinterpret_cast<const void*>(&::tsm::tsm_tn_dmma_kernel<WA, WB, MT, NT, CW, ST, RS>), 0           \
+  }
+
+// Gram C = A^T A on the tensor cores, upper-triangle block pairs (tile fields:
+// the 16 x 16 block pairs it works in).
+#define TSM_GRAM_DMMA_VARIANT(NAME, W, CW, ST, RS)                                                        \
+  ::tsm::Variant {                                                                                       \
+    NAME, ::tsm::kKindDmma, ::tsm::kF64, W, W, 16, 16, 1, ::tsm::GramDmma<W, CW, ST, RS>::THREADS, ST, RS, 1, \
+        ::tsm::GramDmma<W, CW, ST, RS>::SMEM_BYTES,                                                        \
+        reinterpret_cast<const void*>(&::tsm::tsm_gram_dmma_kernel<W, CW, ST, RS>), 1                      \
   }
