@@ -236,10 +236,11 @@ def fp64_gemm_peak(dev) -> dict:
 
 
 def forms(dev) -> dict:
-    """The three forms beside the plain FP64 path, each against FP64 on the
-    same GPU: split precision (n = 2^25, m = k = 32, FP32 storage, column
-    scaled normal data), batched (512 problems, one launch under a CUDA graph
-    vs one plain launch per problem) and differentiation (n = 2^22,
+    """The forms beside the plain FP64 path, each against FP64 on the same
+    GPU: split precision (n = 2^25, m = k = 32, FP32 storage, column scaled
+    normal data), batched (512 problems, one launch under a CUDA graph vs one
+    plain launch per problem), the Gram product C = A^T A (vs the
+    two-operand call on a copy of A) and differentiation (n = 2^22,
     m = k = 16: fused backward vs forward time, FP64 and FP32)."""
     import numpy as np
     import torch
@@ -304,6 +305,24 @@ def forms(dev) -> dict:
                       "err_vs_plain_max_rel": err, "launches": 1, "cuda_graph": True}
     del As, Bs, bt, graph, Cp
     torch.cuda.empty_cache()
+
+    # --- Gram C = A^T A (A streamed once, upper triangle) vs the two-operand
+    #     call on a copy of A
+    rows = []
+    for gm, gn in ((8, 1 << 26), (32, 1 << 26), (64, 1 << 23)):
+        A = torch.empty((gn, gm), dtype=torch.float64, device=dev)
+        tsm.fill_uniform(A, 77, 0)
+        A2 = A.clone()
+        Cg = torch.empty((gm, gm), dtype=torch.float64, device=dev)
+        ms_g = _time(lambda: tsm.gram(A, Cg), 10)
+        ms_p = _time(lambda: tsm.tsmttsm(A, A2, Cg), 10)
+        sym = bool(torch.equal(tsm.gram(A), tsm.gram(A).T))
+        rows.append({"n": gn, "m": gm, "gram_ms": round(ms_g, 4), "two_operand_ms": round(ms_p, 4),
+                     "speedup": round(ms_p / ms_g, 3), "GB/s_of_A": round(8 * gn * gm / (ms_g * 1e-3) / 1e9, 1),
+                     "symmetric": sym})
+        del A, A2
+        torch.cuda.empty_cache()
+    out["gram"] = rows
 
     # --- differentiation: fused backward vs forward
     n, w = 1 << 22, 16
