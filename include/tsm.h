@@ -204,6 +204,18 @@ tsm_status tsm_gemm_tn_backward_f32(tsm_stream_t stream, int64_t n, int m, int k
                                     int64_t ldda, float* dB, int64_t lddb, int beta, void* workspace,
                                     size_t workspace_bytes);
 
+/* Block orthogonalisation against A: C = A^T B (m x k), then B <- B - A C
+ * (in place).  When A has orthonormal columns this removes from B's columns
+ * their components in A's span (one block Gram-Schmidt step); C holds the
+ * projection coefficients.  Two launches on `stream` -- the product, then a
+ * TSMM update (tsm_tsmm_f64 with W = -C, beta = 1) -- reading A twice and B
+ * twice and writing B once; a one-kernel form would still read A twice
+ * and would need a grid-wide wait for C.  A and B must not overlap.
+ * Workspace: tsm_gemm_tn_workspace_size(n, m, k).  No counterpart in the
+ * reference (the fused TSMTTSM + TSMM pipeline). */
+tsm_status tsm_block_orth_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda, double* B,
+                             int64_t ldb, double* C, int64_t ldc, void* workspace, size_t workspace_bytes);
+
 /* ---- Batched products: many C_p = A_p^T B_p (+ C_p) in one launch. ----
  * No counterpart in the reference (it submits one kernel per product; the
  * batching form).  Widths m, k in {4, 8, 16, 32}; A_p, B_p contiguous

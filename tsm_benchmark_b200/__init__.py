@@ -6,7 +6,7 @@ side: ctypes bindings, torch-tensor entry points, the variant generator and
 the autotuner.
 """
 from ._capi import TsmError, TsmLibraryError, variants  # noqa: F401
-from .api import (default_variant, fill_uniform, gram, tsmm, tsmttsm, tsmttsm_backward,  # noqa: F401
+from .api import (block_orthogonalize, default_variant, fill_uniform, gram, tsmm, tsmttsm, tsmttsm_backward,  # noqa: F401
                   tsmttsm_split, workspace_status)
 from .autograd import TSMTTSMFunction, gram_tn  # noqa: F401
 from .batched import BatchedTSMTTSM  # noqa: F401

@@ -99,6 +99,8 @@ SIGNATURES = {
     "tsm_gemm_tn_backward_f32": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                          c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_int,
                                          c_void_p, c_size_t]),
+    "tsm_block_orth_f64": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                   c_void_p, c_int64, c_void_p, c_size_t]),
     "tsm_batched_plan_size_f64": (c_size_t, [c_int, ctypes.POINTER(BatchedProblem)]),
     "tsm_batched_plan_init_f64": (c_int, [c_void_p, c_int, ctypes.POINTER(BatchedProblem), c_void_p, c_size_t,
                                           ctypes.POINTER(BatchedPlan)]),

@@ -123,6 +123,36 @@ def gram(A: torch.Tensor, C: torch.Tensor | None = None, *, accumulate: bool = F
     return C
 
 
+def block_orthogonalize(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *,
+                        stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """C = A^T B, then B <- B - A C in place (FP64; ``tsm_block_orth_f64``):
+    one block Gram-Schmidt step against A's columns when they are
+    orthonormal.  Returns C (m x k), allocated when not given."""
+    _check_operand(A, "A", torch.float64)
+    _check_operand(B, "B", torch.float64)
+    n, m = A.shape
+    k = B.shape[1]
+    if B.shape[0] != n:
+        raise ValueError("A and B must have the same number of rows")
+    if C is None:
+        C = torch.empty((m, k), dtype=torch.float64, device=A.device)
+    else:
+        _check_operand(C, "C", torch.float64)
+        if tuple(C.shape) != (m, k):
+            raise ValueError(f"C must be {m}x{k}, got {tuple(C.shape)}")
+    lib = _capi.load()
+    with torch.cuda.device(A.device):
+        sh = _stream_handle(A.device, stream)
+        need = lib.tsm_gemm_tn_workspace_size(n, m, k)
+        if need == 0:
+            _capi.check(1, "tsm_gemm_tn_workspace_size")
+        ws = workspace(A.device, need, sh)
+        st = lib.tsm_block_orth_f64(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(), _ld(C),
+                                    ws.data_ptr(), ws.numel())
+        _capi.check(st, "tsm_block_orth_f64")
+    return C
+
+
 def default_variant(A: torch.Tensor, B: torch.Tensor) -> int:
     """Index of the variant tsmttsm() would run for these operands."""
     lib = _capi.load()

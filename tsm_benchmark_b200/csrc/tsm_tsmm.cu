@@ -287,6 +287,30 @@ tsm_status tsm_tsmm_f32(tsm_stream_t stream, int64_t n, int p, int q, const floa
   return tsmm_entry<float>(stream, n, p, q, X, ldx, W, w_row, w_col, Y, ldy, beta, workspace, workspace_bytes);
 }
 
+tsm_status tsm_block_orth_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda, double* B,
+                             int64_t ldb, double* C, int64_t ldc, void* workspace, size_t workspace_bytes) {
+  if (B == nullptr && n > 0) return TSM_ERROR_INVALID_VALUE;
+  // 1. C = A^T B.
+  tsm_status s = tsm_gemm_tn_f64(stream, n, m, k, A, lda, B, ldb, C, ldc, 0, workspace, workspace_bytes);
+  if (s != TSM_SUCCESS) return s;
+  // 2. B -= A C: TSMM with X = A (p = m), W = C (m x k, row-major, pitch ldc) read negated, Y = B, beta = 1;
+  //    stream order makes step 1's C visible.
+  TsmmProblem<double> pr{};
+  pr.X = A;
+  pr.ldx = lda;
+  pr.W = C;
+  pr.w_row = ldc;
+  pr.w_col = 1;
+  pr.Y = B;
+  pr.ldy = ldb;
+  pr.n = n;
+  pr.p = m;
+  pr.q = k;
+  pr.beta = 1;
+  pr.negate = 1;
+  return launch_tsmm<double>(static_cast<cudaStream_t>(stream), &pr, 1, workspace, workspace_bytes);
+}
+
 tsm_status tsm_gemm_tn_backward_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
                                     const double* B, int64_t ldb, const double* dC, int64_t lddc, double* dA,
                                     int64_t ldda, double* dB, int64_t lddb, int beta, void* workspace,

@@ -38,6 +38,7 @@ struct TsmmProblem {
   int64_t n;
   int p, q;
   int beta;            // 0: Y = X W, 1: Y += X W
+  int negate;          // 1: W is read as -W (exact), so beta = 1 gives Y -= X W
   int64_t rows_main;   // rows the TMA ring streams; the rest are read directly
   int64_t num_chunks;  // ceil(rows_main / RS)
 };
@@ -56,9 +57,11 @@ namespace detail {
 template <typename T, int C>
 __device__ __forceinline__ void load_w_column(const TsmmProblem<T>& pr, int o, T (&w)[C]) {
 #pragma unroll
-  for (int a = 0; a < C; ++a)
-    w[a] = (a < pr.p && o < pr.q) ? pr.W[static_cast<int64_t>(a) * pr.w_row + static_cast<int64_t>(o) * pr.w_col]
-                                  : T(0);
+  for (int a = 0; a < C; ++a) {
+    const T x = (a < pr.p && o < pr.q) ? pr.W[static_cast<int64_t>(a) * pr.w_row + static_cast<int64_t>(o) * pr.w_col]
+                                       : T(0);
+    w[a] = pr.negate ? -x : x;
+  }
 }
 
 // y = x_row . w for one row held in memory at `x` (p valid elements).

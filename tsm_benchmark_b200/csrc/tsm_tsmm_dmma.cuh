@@ -84,10 +84,11 @@ __device__ __forceinline__ void load_w_frags(const TsmmProblem<TX>& pr, int o0, 
 #pragma unroll
     for (int j = 0; j < NT; ++j) {
       const int o = o0 + 8 * j + g;
-      b[s][j] = (kappa < pr.p && o < pr.q)
-                    ? static_cast<double>(
-                          pr.W[static_cast<int64_t>(kappa) * pr.w_row + static_cast<int64_t>(o) * pr.w_col])
-                    : 0.0;
+      const double w = (kappa < pr.p && o < pr.q)
+                           ? static_cast<double>(
+                                 pr.W[static_cast<int64_t>(kappa) * pr.w_row + static_cast<int64_t>(o) * pr.w_col])
+                           : 0.0;
+      b[s][j] = pr.negate ? -w : w;
     }
   }
 }
@@ -313,6 +314,7 @@ __global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>::THRE
             y = fma(static_cast<double>(pr.X[r * pr.ldx + a]),
                     static_cast<double>(pr.W[static_cast<int64_t>(a) * pr.w_row + static_cast<int64_t>(o) * pr.w_col]),
                     y);
+          if (pr.negate) y = -y;
           detail::store_y(pr, r, o, static_cast<TX>(y));
         }
       }
