@@ -165,13 +165,24 @@ def reference_cpu(n_sample: int, steps: int, warmup: int, budget_s: float) -> di
         times.append(run())
         if time.perf_counter() - t_start > budget_s and len(times) >= 1:
             break
-    ref_c = oracle.naive(A[: min(n_sample, 1 << 16)], B[: min(n_sample, 1 << 16)])  # noqa: F841 (sanity only)
     t = sum(times) / len(times)
     gbs = algo_bytes(n_sample, HEAD_M, HEAD_K) / t / 1e9
+    # The reference's own FP64 oracle, compute_naive (main.cc:14-27), one
+    # thread, on the first 2^20 rows (one run).
+    naive = None
+    if R is not None:
+        nn = min(n_sample, 1 << 20)
+        Cn = __import__("numpy").zeros(HEAD_M * HEAD_K)
+        t0 = time.perf_counter()
+        R.ref_compute_naive_f64(nn, HEAD_M, p(A), p(B), p(Cn))
+        tn = time.perf_counter() - t0
+        naive = {"value": algo_bytes(nn, HEAD_M, HEAD_K) / tn / 1e9, "unit": "GB/s", "cores": 1,
+                 "sample": f"compute_naive, n={nn} rows x m=k=8, one run of {tn * 1e3:.1f} ms"}
     return {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind, "steps_timed": len(times),
             "sample": (f"n={n_sample} rows x m=k=8 (the headline shape at {n_sample / HEAD_N:.4g} of its rows), "
                        f"tsmttsm4 stride {REF_STRIDE} tile {REF_TILE}, mean of {len(times)} runs "
-                       f"of {t * 1e3:.1f} ms")}
+                       f"of {t * 1e3:.1f} ms"),
+            "naive_single_core": naive}
 
 
 def run_reference_arm(args) -> None:
@@ -544,7 +555,7 @@ def main() -> int:
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         res = reference_cpu(args.ref_rows, steps=50, warmup=1, budget_s=args.ref_budget)
-        cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample", "naive_single_core")}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
