@@ -223,7 +223,7 @@ class DmmaVariant:
     @property
     def regions(self) -> int:
         if self.gram:  # upper-triangle block-pair regions of tsm_gram_dmma_kernel
-            return {16: 1, 32: 1, 48: 2, 64: 3}[self.wa]
+            return {16: 1, 32: 1, 48: 2, 64: 2}[self.wa]
         mt, nt = (self.mt, self.nt) if self.mt else self.best_region(self.wa, self.wb)
         return ((self.wa // 8) // mt) * ((self.wb // 8) // nt)
 

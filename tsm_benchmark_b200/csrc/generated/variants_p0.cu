@@ -39,7 +39,7 @@ const Variant kGenPart0[] = {
     TSM_DIRECT_VARIANT("directf32_16x1_t8x1_th256_cap", float, 16, 1, 8, 1, 256, false),
     TSM_DIRECT_VARIANT("directf32_32x2_t8x2_th256_cap", float, 32, 2, 8, 2, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x4_t8x4_th256_cap", float, 64, 4, 8, 4, 256, false),
-    TSM_GRAM_DMMA_VARIANT("dmma_64x64_gram_w9_s3_r120", 64, 9, 3, 120),
+    TSM_GRAM_DMMA_VARIANT("dmma_64x64_gram_w8_s3_r128", 64, 8, 3, 128),
 };
 extern const int kGenPart0Count;
 const int kGenPart0Count = 33;

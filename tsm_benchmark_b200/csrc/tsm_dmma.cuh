@@ -230,24 +230,23 @@ namespace tsm {
 // triangle is complete and the lower one is written by mirroring
 // (finish_partials with symmetric = 1).  Per k-step a warp loads each 16-column
 // block its region touches ONCE and feeds both DMMA operands from it (B is A).
-// Regions (lists of block pairs, <= 16 tiles):
-//   W = 16: {(0,0)}                              1 region
-//   W = 32: {(0,0),(0,1),(1,1)}                  1 region, 12 of 16 tiles
-//   W = 48: {(0,0),(0,1),(1,1)}, {(0,2),(1,2),(2,2)}           24 of 36 tiles
-//   W = 64: {(0,0),(0,1),(1,1)}, {(2,2),(2,3),(3,3)},
-//           {(0,2),(0,3),(1,2),(1,3)}                          40 of 64 tiles
+// Regions (lists of block pairs, equal tile counts, <= 20 tiles):
+//   W = 16: {(0,0)}                                         1 region
+//   W = 32: {(0,0),(0,1),(1,1)}                             1 region, 12 of 16 tiles
+//   W = 48: {(0,0),(0,1),(1,1)}, {(0,2),(1,2),(2,2)}        24 of 36 tiles
+//   W = 64: {(0,0),(0,1),(0,2),(0,3),(1,1)},
+//           {(1,2),(1,3),(2,2),(2,3),(3,3)}                 40 of 64 tiles
 // A pair is coded 4 bi + bj, four bits per pair.
-__host__ __device__ constexpr int gram_regions(int W) { return W == 64 ? 3 : (W == 48 ? 2 : 1); }
-__host__ __device__ constexpr int gram_npairs(int W, int r) {
-  return W == 16 ? 1 : (W == 64 && r == 2 ? 4 : 3);
-}
+__host__ __device__ constexpr int gram_regions(int W) { return W >= 48 ? 2 : 1; }
+__host__ __device__ constexpr int gram_npairs(int W, int) { return W == 16 ? 1 : (W == 64 ? 5 : 3); }
 __host__ __device__ constexpr unsigned gram_pair_codes(int W, int r) {
-  return W == 16 ? 0x0u
-         : r == 0 ? (0x0u | (0x1u << 4) | (0x5u << 8))
-         : (W == 48 || r == 2) ? (W == 48 ? (0x2u | (0x6u << 4) | (0xAu << 8))
-                                          : (0x2u | (0x3u << 4) | (0x6u << 8) | (0x7u << 12)))
-                               : (0xAu | (0xBu << 4) | (0xFu << 8));
+  return W == 16   ? 0x0u
+         : W == 32 ? (0x0u | (0x1u << 4) | (0x5u << 8))
+         : W == 48 ? (r == 0 ? (0x0u | (0x1u << 4) | (0x5u << 8)) : (0x2u | (0x6u << 4) | (0xAu << 8)))
+         : r == 0  ? (0x0u | (0x1u << 4) | (0x2u << 8) | (0x3u << 12) | (0x5u << 16))
+                   : (0x6u | (0x7u << 4) | (0xAu << 8) | (0xBu << 12) | (0xFu << 16));
 }
+constexpr int kGramMaxPairs = 5;
 __host__ __device__ constexpr int gram_pair(int W, int r, int p) {
   return static_cast<int>((gram_pair_codes(W, r) >> (4 * p)) & 0xFu);
 }
@@ -284,14 +283,14 @@ namespace detail {
 template <int W, int CW, int STAGES, int RS, int REG>
 __device__ __forceinline__ void gram_consume(const PlainArgs<double>& p, unsigned char* smem, uint64_t* full,
                                              uint64_t* empty, volatile int* abort, int slot, int lane,
-                                             double (&out)[4][2][2][2]) {
+                                             double (&out)[kGramMaxPairs][2][2][2]) {
   using K = GramDmma<W, CW, STAGES, RS>;
   constexpr int NP = gram_npairs(W, REG);
   constexpr unsigned MASK = gram_block_mask(W, REG);
   const int g = lane >> 2, tq = lane & 3;
   const int64_t G = gridDim.x;
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
+  for (int q = 0; q < kGramMaxPairs; ++q)
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -337,7 +336,7 @@ __device__ __forceinline__ void gram_consume(const PlainArgs<double>& p, unsigne
 // Tile (pair q, parities a, b) -> C row 16 bi + 2 g + a, column 16 bj + 2 n + b
 // for D column n = 2 tq + e.
 template <int W, int REG>
-__device__ __forceinline__ void gram_store(double* sheet, int lane, const double (&out)[4][2][2][2]) {
+__device__ __forceinline__ void gram_store(double* sheet, int lane, const double (&out)[kGramMaxPairs][2][2][2]) {
   constexpr int NP = gram_npairs(W, REG);
   const int g = lane >> 2, tq = lane & 3;
 #pragma unroll
@@ -382,7 +381,7 @@ __global__ void __launch_bounds__(GramDmma<W, CW, STAGES, RS>::THREADS, 1)
 
   const int64_t G = gridDim.x;
   const int region = warp % K::R, slot = warp / K::R;
-  double out[4][2][2][2];
+  double out[kGramMaxPairs][2][2][2];
 
   if (warp == CW) {
     // ---------------- producer warp: A's boxes only.
@@ -411,10 +410,8 @@ __global__ void __launch_bounds__(GramDmma<W, CW, STAGES, RS>::THREADS, 1)
     }
   } else if (region == 0) {
     detail::gram_consume<W, CW, STAGES, RS, 0>(p, smem, full, empty, abort, slot, lane, out);
-  } else if (region == 1) {
-    detail::gram_consume<W, CW, STAGES, RS, (K::R > 1 ? 1 : 0)>(p, smem, full, empty, abort, slot, lane, out);
   } else {
-    detail::gram_consume<W, CW, STAGES, RS, (K::R > 2 ? 2 : 0)>(p, smem, full, empty, abort, slot, lane, out);
+    detail::gram_consume<W, CW, STAGES, RS, (K::R > 1 ? 1 : 0)>(p, smem, full, empty, abort, slot, lane, out);
   }
 
   __syncthreads();
@@ -434,10 +431,8 @@ __global__ void __launch_bounds__(GramDmma<W, CW, STAGES, RS>::THREADS, 1)
     double* sheet = red + slot * (W * W);
     if (region == 0)
       detail::gram_store<W, 0>(sheet, lane, out);
-    else if (region == 1)
-      detail::gram_store<W, (K::R > 1 ? 1 : 0)>(sheet, lane, out);
     else
-      detail::gram_store<W, (K::R > 2 ? 2 : 0)>(sheet, lane, out);
+      detail::gram_store<W, (K::R > 1 ? 1 : 0)>(sheet, lane, out);
   }
   __syncthreads();
   detail::finish_partials(p, red, K::S, t, K::THREADS, s_is_last);
