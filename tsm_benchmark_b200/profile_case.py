@@ -3,7 +3,7 @@
 under a profiler (ncu) or to time one variant.
 
     python -m tsm_benchmark_b200.profile_case --n 4194304 --m 8 --k 8 --reps 4 [--variant NAME]
-    python -m tsm_benchmark_b200.profile_case --form split|backward --n ... --m ... --k ...
+    python -m tsm_benchmark_b200.profile_case --form split|backward|gram|batched --n ... --m ... --k ...
 
 One untimed call comes first (library setup); a profiler capture of the k-th
 timed launch therefore skips k launches (`ncu -s k`).
@@ -28,13 +28,45 @@ def main(argv=None) -> int:
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--reps", type=int, default=4)
     ap.add_argument("--variant", default=None, help="variant name (default: the library's choice)")
-    ap.add_argument("--form", choices=["plain", "split", "backward"], default="plain",
-                    help="plain FP64, FP32 TF32-split on tensor cores, or the fused backward")
+    ap.add_argument("--form", choices=["plain", "split", "backward", "gram", "batched"], default="plain",
+                    help="plain FP64, FP32 TF32-split on tensor cores, the fused backward, the Gram product "
+                         "C = A^T A, or a batch of --count products of n rows and widths m x k in one launch")
+    ap.add_argument("--count", type=int, default=64, help="problems in the batch (--form batched)")
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64", help="storage type of the backward")
     args = ap.parse_args(argv)
 
-    from tsm_benchmark_b200 import fill_uniform, tsmttsm, tsmttsm_backward, tsmttsm_split, variants
+    from tsm_benchmark_b200 import (BatchedTSMTTSM, fill_uniform, gram, tsmttsm, tsmttsm_backward, tsmttsm_split,
+                                    variants)
     dev = torch.device("cuda", 0)
+    if args.form in ("gram", "batched"):
+        if args.form == "gram":
+            A = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
+            fill_uniform(A, 1, 0)
+            run = lambda: gram(A)  # noqa: E731
+            nbytes = 8 * args.n * args.m
+        else:
+            As, Bs = [], []
+            for i in range(args.count):
+                a = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
+                b = torch.empty((args.n, args.k), dtype=torch.float64, device=dev)
+                fill_uniform(a, 10 + i, 0)
+                fill_uniform(b, 10 + i, 1)
+                As.append(a)
+                Bs.append(b)
+            bt = BatchedTSMTTSM(As, Bs)
+            run = bt.run
+            nbytes = 8 * args.count * args.n * (args.m + args.k)
+        run()  # first call: library setup, not timed
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(args.reps):
+            run()
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.reps
+        print(f"{args.form} n={args.n} m={args.m} k={args.k}: {ms:.4f} ms/call, {nbytes / (ms * 1e-3) / 1e9:.1f} GB/s")
+        return 0
     if args.form != "plain":
         A = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
         B = torch.empty((args.n, args.k), dtype=torch.float64, device=dev)
