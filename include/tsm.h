@@ -141,6 +141,16 @@ tsm_status tsm_variant_get_info(int index, tsm_variant_info* info);
  * not valid; the call then returns TSM_ERROR_DEVICE_TIMEOUT. */
 tsm_status tsm_workspace_check(tsm_stream_t stream, void* workspace, unsigned* bits);
 
+/* Self-test of the device failure path: launches one kernel whose wait on
+ * an mbarrier that nothing arrives on runs out after limit_us microseconds
+ * (1 .. 2,000,000) -- through the same bounded wait every pipeline uses --
+ * and records the timeout in the workspace's error word.  A following
+ * tsm_workspace_check returns TSM_ERROR_DEVICE_TIMEOUT and clears the word;
+ * the context stays usable.  No fault, no trap.  No counterpart in the
+ * reference (it has no failure detection). */
+tsm_status tsm_selftest_wait_timeout(tsm_stream_t stream, void* workspace, size_t workspace_bytes,
+                                     unsigned limit_us);
+
 /* C = A^T A (accumulate = 0) or C += A^T A, FP64: the Gram matrix of a tall
  * and skinny A (n x m, pitch lda).  Reads A once -- half the bytes of
  * tsm_gemm_tn_f64 on two operands -- and writes C exactly symmetric (each

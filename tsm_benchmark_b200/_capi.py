@@ -87,6 +87,7 @@ SIGNATURES = {
     "tsm_gemm_tn_default_variant": (c_int, [c_int, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64]),
     "tsm_variant_count": (c_int, []),
     "tsm_variant_get_info": (c_int, [c_int, ctypes.POINTER(VariantInfo)]),
+    "tsm_selftest_wait_timeout": (c_int, [c_void_p, c_void_p, c_size_t, ctypes.c_uint]),
     "tsm_workspace_check": (c_int, [c_void_p, c_void_p, ctypes.POINTER(ctypes.c_uint)]),
     "tsm_fill_uniform_f64": (c_int, [c_void_p, c_void_p, c_int64, c_uint64, c_uint64]),
     "tsm_tsmm_f64": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_int64,

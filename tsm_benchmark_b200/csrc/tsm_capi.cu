@@ -299,6 +299,22 @@ tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const T* A
   return launch_variant(v, p, grid, stream);
 }
 
+// ------------------------------------------------------- timeout self-test
+// One thread waits on an mbarrier that nothing ever arrives on, through the
+// same bounded wait every pipeline uses, then records the timeout in the
+// workspace's error word -- the failure path of the kernels, exercised on
+// purpose (a wait that runs out; no fault, no trap).
+__global__ void selftest_wait_kernel(unsigned* error, uint64_t limit_ns) {
+  __shared__ uint64_t bar;
+  __shared__ int abort;
+  if (threadIdx.x == 0) {
+    dev::mbar_init(&bar, 1);
+    abort = 0;
+    dev::fence_mbar_init();
+    if (!dev::mbar_wait_for(&bar, 0, &abort, limit_ns)) atomicOr(error, dev::kErrTimeout);
+  }
+}
+
 // ----------------------------------------------------------------- fills
 __global__ void fill_uniform_kernel(double* x, int64_t count, uint64_t seed, uint64_t stream_id) {
   const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -405,6 +421,17 @@ tsm_status tsm_variant_get_info(int index, tsm_variant_info* info) {
   info->unroll = v->unroll;
   info->smem_bytes = v->smem;
   info->gram = v->gram;
+  return TSM_SUCCESS;
+}
+
+tsm_status tsm_selftest_wait_timeout(tsm_stream_t stream, void* workspace, size_t workspace_bytes,
+                                     unsigned limit_us) {
+  if (workspace == nullptr || workspace_bytes < kWsHeader || !aligned16(workspace)) return TSM_ERROR_WORKSPACE;
+  if (limit_us == 0 || limit_us > 2000000u) return TSM_ERROR_INVALID_VALUE;
+  unsigned* error = reinterpret_cast<unsigned*>(workspace) + 1;
+  selftest_wait_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(error, uint64_t(limit_us) * 1000u);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "selftest_wait_kernel");
   return TSM_SUCCESS;
 }
 
