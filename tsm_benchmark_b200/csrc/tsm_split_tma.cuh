@@ -24,9 +24,11 @@
 // stage to its lo stage as the leading byte offset (LBO) between the hi and
 // lo atoms of an operand.
 //
-// Warp roles (14 warps): 0 producer, 1 TMEM owner + MMA issuer, 2-9
-// converters, 10-13 epilogue (TMEM -> FP64 sums, double-buffered
-// accumulators).  All waits are bounded (dev::mbar_wait); on a timeout the CTA
+// Warp roles (15 warps): 0 producer, 1 TMEM owner + MMA issuer of the even
+// chunks, 14 MMA issuer of the odd chunks (issuing tcgen05.mma from one
+// thread was a measured bottleneck; each issuer owns one lo stage and one
+// TMEM accumulator, so they share no barrier phase), 2-9 converters, 10-13
+// epilogue (TMEM -> FP64 sums).  All waits are bounded (dev::mbar_wait); on a timeout the CTA
 // records the error, drains its copies and MMAs (bounded) and frees its TMEM.
 #pragma once
 
@@ -56,7 +58,8 @@ constexpr int kStageBytes = 2 * kTileBytes;  // A part, B part
 constexpr int kLoRing = kHiStages * kStageBytes;  // offset of the lo ring
 constexpr int kConvWarps = 8;
 constexpr int kEpiWarp0 = 10;
-constexpr int kWarps = 14;
+constexpr int kMma2Warp = 14;  // second MMA issuer (odd chunks)
+constexpr int kWarps = 15;
 constexpr int kThreads = kWarps * 32;
 constexpr int kTmemCols = 128;  // two 64-column accumulators
 constexpr uint32_t kIdesc = dev::umma_idesc_tf32(64, 64, true, true);
@@ -158,10 +161,13 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
     }
-  } else if (warp == 1) {
-    // ---------------- MMA issuer (lane 0); the warp stays converged.
+  } else if (warp == 1 || warp == kMma2Warp) {
+    // ---------------- MMA issuers (lane 0): warp 1 the even chunks, warp 14
+    // the odd ones; the warp stays converged.
+    static_assert(kLoStages == 2, "one lo stage and one accumulator per issuer");
     const uint32_t base = dev::smem_u32(smem);
-    for (int64_t it = 0; it < nchunks_mine; ++it) {
+    const int64_t parity = warp == 1 ? 0 : 1;
+    for (int64_t it = parity; it < nchunks_mine; it += 2) {
       const int s = static_cast<int>(it % kHiStages);
       const int o = static_cast<int>(it % kLoStages);
       const int b = static_cast<int>(it & 1);
