@@ -24,12 +24,15 @@
 // stage to its lo stage as the leading byte offset (LBO) between the hi and
 // lo atoms of an operand.
 //
-// Warp roles (15 warps): 0 producer, 1 TMEM owner + MMA issuer of the even
-// chunks, 14 MMA issuer of the odd chunks (issuing tcgen05.mma from one
-// thread was a measured bottleneck; each issuer owns one lo stage and one
-// TMEM accumulator, so they share no barrier phase), 2-9 converters, 10-13
-// epilogue (TMEM -> FP64 sums).  All waits are bounded (dev::mbar_wait); on a timeout the CTA
-// records the error, drains its copies and MMAs (bounded) and frees its TMEM.
+// Warp roles (16 warps): 0 producer, 1 TMEM owner + MMA issuer of chunks
+// 0, 3, 6 .., 14 and 15 MMA issuers of chunks 1, 4 .. and 2, 5 .. (issuing
+// tcgen05.mma from one thread was a measured bottleneck: 2^25 x 32 x 32 took
+// 1.79 ms with one issuer, 1.56 with two, 1.53 with three; each issuer owns
+// one lo stage and one TMEM accumulator, so they share no barrier phase),
+// 2-9 converters, 10-13 epilogue (TMEM -> FP64 sums).  A fourth issuer (17
+// warps, three hi stages) drops the register cap to 96 and spills.  All
+// waits are bounded (dev::mbar_wait); on a timeout the CTA records the
+// error, drains its copies and MMAs (bounded) and frees its TMEM.
 #pragma once
 
 #include <cuda.h>
@@ -51,24 +54,27 @@ struct SplitTmaArgs {
 namespace split2 {
 
 constexpr int kRows = 128;                   // rows per chunk (16 MMAs of K = 8)
-constexpr int kHiStages = 5;
-constexpr int kLoStages = 2;
+// kIssuers warps issue the MMAs (chunk it goes to issuer it % kIssuers);
+// each owns one lo stage and one TMEM accumulator.
+constexpr int kIssuers = 3;
+constexpr int kHiStages = kIssuers == 2 ? 5 : 4;
+constexpr int kLoStages = kIssuers;
 constexpr int kTileBytes = kRows * 128;      // one operand part: 32 floats x 128 rows
 constexpr int kStageBytes = 2 * kTileBytes;  // A part, B part
 constexpr int kLoRing = kHiStages * kStageBytes;  // offset of the lo ring
 constexpr int kConvWarps = 8;
 constexpr int kEpiWarp0 = 10;
-constexpr int kMma2Warp = 14;  // second MMA issuer (odd chunks)
-constexpr int kWarps = 15;
+constexpr int kWarps = 13 + kIssuers;  // issuers: warp 1, then warps 14 ..
 constexpr int kThreads = kWarps * 32;
-constexpr int kTmemCols = 128;  // two 64-column accumulators
+constexpr int kTmemCols = kIssuers * 64 <= 128 ? 128 : 256;  // one 64-column accumulator per issuer
 constexpr uint32_t kIdesc = dev::umma_idesc_tf32(64, 64, true, true);
 constexpr size_t kBarOffset = size_t(kLoRing) + size_t(kLoStages) * kStageBytes;
-constexpr int kNumBars = 2 * kHiStages + 2 * kLoStages + 4;
+constexpr int kNumBars = 2 * kHiStages + 2 * kLoStages + 2 * kIssuers;
 constexpr size_t kSmemBytes = kBarOffset + kNumBars * 8 + 32 + 1024;  // + alignment slack
 static_assert(kTileBytes % 1024 == 0, "tiles keep the 1024-byte alignment of the swizzle atoms");
 static_assert((kLoRing + (kLoStages - 1) * kStageBytes) / 16 < (1 << 14), "LBO must fit the descriptor field");
 static_assert(kSmemBytes <= 232448, "dynamic shared memory limit of sm_100a");
+static_assert(kIssuers == 2 || kIssuers == 3, "four issuers (17 warps) spill the epilogue sums");
 
 // lo part of x: x - trunc_tf32(x) (exact) rounded to nearest TF32, ties away
 // from zero (add half a TF32 unit to the magnitude bits, clear 13 bits).
@@ -93,7 +99,7 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
   uint64_t* lo_full = empty + kHiStages;     // lo stage written (converter warps)
   uint64_t* lo_empty = lo_full + kLoStages;  // lo stage's MMAs completed (commit)
   uint64_t* d_full = lo_empty + kLoStages;   // accumulator b complete (commit)
-  uint64_t* d_empty = d_full + 2;            // accumulator b drained (epilogue warps)
+  uint64_t* d_empty = d_full + kIssuers;     // accumulator b drained (epilogue warps)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kNumBars);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
   unsigned* s_is_last = reinterpret_cast<unsigned*>(tmem_slot + 2);
@@ -111,7 +117,7 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       dev::mbar_init(&lo_full[o], kConvWarps);
       dev::mbar_init(&lo_empty[o], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kIssuers; ++b) {
       dev::mbar_init(&d_full[b], 1);
       dev::mbar_init(&d_empty[b], 4);
     }
@@ -161,20 +167,20 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
     }
-  } else if (warp == 1 || warp == kMma2Warp) {
-    // ---------------- MMA issuers (lane 0): warp 1 the even chunks, warp 14
-    // the odd ones; the warp stays converged.
-    static_assert(kLoStages == 2, "one lo stage and one accumulator per issuer");
+  } else if (warp == 1 || warp >= 14) {
+    // ---------------- MMA issuers (lane 0): issuer r (warp 1, then 14 ..)
+    // takes the chunks it = r mod kIssuers; the warp stays converged.
     const uint32_t base = dev::smem_u32(smem);
-    const int64_t parity = warp == 1 ? 0 : 1;
-    for (int64_t it = parity; it < nchunks_mine; it += 2) {
+    const int64_t first = warp == 1 ? 0 : warp - 13;
+    for (int64_t it = first; it < nchunks_mine; it += kIssuers) {
       const int s = static_cast<int>(it % kHiStages);
       const int o = static_cast<int>(it % kLoStages);
-      const int b = static_cast<int>(it & 1);
+      const int b = static_cast<int>(it % kIssuers);
       bool ok = true;
       if (lane == 0) {
         ok = dev::mbar_wait(&lo_full[o], static_cast<uint32_t>((it / kLoStages) & 1), abort);
-        if (ok && it >= 2) ok = dev::mbar_wait(&d_empty[b], static_cast<uint32_t>(((it >> 1) - 1) & 1), abort);
+        if (ok && it >= kIssuers)
+          ok = dev::mbar_wait(&d_empty[b], static_cast<uint32_t>(((it / kIssuers) - 1) & 1), abort);
         if (ok) {
           dev::tc_fence_after();
           const uint32_t a_base = base + s * kStageBytes;
@@ -233,8 +239,8 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
     const int q = warp & 3;
     const uint32_t lane_base = static_cast<uint32_t>(32 * q) << 16;
     for (int64_t it = 0; it < nchunks_mine; ++it) {
-      const int b = static_cast<int>(it & 1);
-      if (!dev::mbar_wait(&d_full[b], static_cast<uint32_t>((it >> 1) & 1), abort)) {
+      const int b = static_cast<int>(it % kIssuers);
+      if (!dev::mbar_wait(&d_full[b], static_cast<uint32_t>((it / kIssuers) & 1), abort)) {
         *abort = 1;
         atomicOr(p.error, dev::kErrTimeout);
         break;
@@ -267,8 +273,8 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       for (int64_t it = nchunks_mine > kHiStages ? nchunks_mine - kHiStages : 0; it < nchunks_mine; ++it)
         if (!dev::mbar_wait(&full[it % kHiStages], static_cast<uint32_t>((it / kHiStages) & 1), &no_abort)) break;
     } else if (warp == 1) {
-      for (int64_t it = nchunks_mine > 2 ? nchunks_mine - 2 : 0; it < nchunks_mine; ++it)
-        if (!dev::mbar_wait(&d_full[it & 1], static_cast<uint32_t>((it >> 1) & 1), &no_abort)) break;
+      for (int64_t it = nchunks_mine > kIssuers ? nchunks_mine - kIssuers : 0; it < nchunks_mine; ++it)
+        if (!dev::mbar_wait(&d_full[it % kIssuers], static_cast<uint32_t>((it / kIssuers) & 1), &no_abort)) break;
     }
   }
   dev::tc_fence_before();
