@@ -161,6 +161,24 @@ tsm_status tsm_selftest_wait_timeout(tsm_stream_t stream, void* workspace, size_
 tsm_status tsm_gram_f64(tsm_stream_t stream, int64_t n, int m, const double* A, int64_t lda, double* C, int64_t ldc,
                         int accumulate, void* workspace, size_t workspace_bytes);
 
+/* C = A^T B (accumulate = 0) or C += A^T B, FP64, for operands in any
+ * element layout: A's element (r, i), r < n, i < m, is A[r * a_row + i *
+ * a_col] and B's (r, j) is B[r * b_row + j * b_col]; every stride >= 1.
+ * Row-major operands (a_col = b_col = 1, a_row >= m, b_row >= k) take the
+ * tsm_gemm_tn_f64 path.  Column-major operands (a_row = b_row = 1: A stored
+ * as the m x n row-major matrix A^T with pitch a_col >= n, B likewise) stream
+ * through tensor maps when the bases are 16-byte aligned and the pitches even
+ * (values of r contiguous, columns zero-padded to the kernel's capacity);
+ * FP64 tensor cores when the widths rounded up to powers of two multiply to
+ * more than 64.  Any other layout (mixed, odd pitches, unaligned) runs a
+ * register-tile kernel with strided loads: correct, not tuned.  No
+ * counterpart in the reference, whose operands are always row-major with
+ * pitch M (tsmttsm.hh:15-35; sycl_codegen_new.py:66-67).  Same workspace as
+ * tsm_gemm_tn_f64 (tsm_gemm_tn_workspace_size(n, m, k)). */
+tsm_status tsm_gemm_tn_strided_f64(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t a_row,
+                                   int64_t a_col, const double* B, int64_t b_row, int64_t b_col, double* C,
+                                   int64_t ldc, int accumulate, void* workspace, size_t workspace_bytes);
+
 /* C = A^T B (accumulate = 0) or C += A^T B (accumulate = 1), FP64, WITHOUT a
  * workspace.  No counterpart in the reference (its SYCL kernels need no
  * scratch because they add into C with atomics).  For callers that cannot

@@ -76,6 +76,8 @@ SIGNATURES = {
                                 c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gram_f64": (c_int, [c_void_p, c_int64, c_int, c_void_p, c_int64, c_void_p, c_int64, c_int, c_void_p,
                              c_size_t]),
+    "tsm_gemm_tn_strided_f64": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_int64, c_void_p,
+                                        c_int64, c_int64, c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_f64_variant": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int, c_void_p, c_size_t, c_int]),
     "tsm_gemm_tn_f32": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,

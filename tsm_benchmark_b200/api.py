@@ -2,7 +2,9 @@
 
 torch is used for device memory and streams only; every computation is a
 call into libtsm_b200.so.  Shapes follow include/tsm.h: A (n x m), B (n x k)
-row-major (unit column stride, any row stride), C (m x k).
+row-major (unit column stride, any row stride), C (m x k); FP64 operands
+in other layouts (column-major ``X.T`` views included) go through
+``tsm_gemm_tn_strided_f64``.
 """
 from __future__ import annotations
 
@@ -34,15 +36,29 @@ def workspace(device: torch.device, nbytes: int, stream_handle: int) -> torch.Te
         return ws
 
 
-def _check_operand(x: torch.Tensor, name: str, dtype: torch.dtype) -> None:
+def _check_operand(x: torch.Tensor, name: str, dtype: torch.dtype, any_strides: bool = False) -> None:
     if not x.is_cuda:
         raise ValueError(f"{name} must be a CUDA tensor (there is no CPU path)")
     if x.dtype != dtype:
         raise TypeError(f"{name} must be {dtype}, got {x.dtype}")
     if x.dim() != 2:
         raise ValueError(f"{name} must be 2-D, got shape {tuple(x.shape)}")
-    if x.shape[0] > 0 and x.shape[1] > 1 and x.stride(1) != 1:
+    if not any_strides and x.shape[0] > 0 and x.shape[1] > 1 and x.stride(1) != 1:
         raise ValueError(f"{name} must have unit column stride (row-major rows)")
+
+
+def _row_major(x: torch.Tensor) -> bool:
+    return x.shape[0] == 0 or x.shape[1] == 1 or x.stride(1) == 1
+
+
+def _strides(x: torch.Tensor) -> tuple[int, int]:
+    """(row stride, column stride) in elements, >= 1: strides along an
+    extent of one carry no layout and are reported as 1."""
+    r = int(x.stride(0)) if x.shape[0] > 1 else 1
+    c = int(x.stride(1)) if x.shape[1] > 1 else 1
+    if r < 1 or c < 1:
+        raise ValueError("operands need positive strides (no broadcast or reversed views)")
+    return r, c
 
 
 def _ld(x: torch.Tensor) -> int:
@@ -61,13 +77,17 @@ def tsmttsm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, 
     The Python face of ``tsm_gemm_tn_f64`` / ``tsm_gemm_tn_f32`` (the
     reference's ``tsmttsm*<double, M, ...>(q, K, A, B, C)``,
     tsmttsm.hh:15-586, which always accumulates).  A, B and C share one
-    dtype.  Returns C; allocates it (m x k) when not given.
+    dtype.  FP64 operands may have any positive strides: column-major ones
+    (``X.T`` of a row-major m x n X) and mixed layouts run through
+    ``tsm_gemm_tn_strided_f64`` (``variant`` is then ignored).  Returns C;
+    allocates it (m x k) when not given.
     """
     if A.dtype not in _PLAIN:
         raise TypeError(f"A must be float64 or float32, got {A.dtype}")
     fn_name, _ = _PLAIN[A.dtype]
-    _check_operand(A, "A", A.dtype)
-    _check_operand(B, "B", A.dtype)
+    f64 = A.dtype == torch.float64
+    _check_operand(A, "A", A.dtype, any_strides=f64)
+    _check_operand(B, "B", A.dtype, any_strides=f64)
     if A.shape[0] != B.shape[0]:
         raise ValueError(f"A and B must have the same number of rows, got {A.shape[0]} and {B.shape[0]}")
     if A.device != B.device:
@@ -89,9 +109,15 @@ def tsmttsm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, 
         if need == 0:
             _capi.check(1, "tsm_gemm_tn_workspace_size")
         ws = workspace(A.device, need, sh)
-        st = getattr(lib, fn_name)(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
-                                   _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel(), int(variant))
-        _capi.check(st, fn_name)
+        if _row_major(A) and _row_major(B):
+            st = getattr(lib, fn_name)(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
+                                       _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel(), int(variant))
+            _capi.check(st, fn_name)
+        else:
+            (ar, ac), (br, bc) = _strides(A), _strides(B)
+            st = lib.tsm_gemm_tn_strided_f64(sh, n, m, k, A.data_ptr(), ar, ac, B.data_ptr(), br, bc, C.data_ptr(),
+                                             _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel())
+            _capi.check(st, "tsm_gemm_tn_strided_f64")
     return C
 
 

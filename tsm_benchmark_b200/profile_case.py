@@ -4,6 +4,7 @@ under a profiler (ncu) or to time one variant.
 
     python -m tsm_benchmark_b200.profile_case --n 4194304 --m 8 --k 8 --reps 4 [--variant NAME]
     python -m tsm_benchmark_b200.profile_case --form split|backward|gram|batched --n ... --m ... --k ...
+    python -m tsm_benchmark_b200.profile_case --layout col --n ... --m ... --k ...   (A^T, B^T row-major)
 
 One untimed call comes first (library setup); a profiler capture of the k-th
 timed launch therefore skips k launches (`ncu -s k`).
@@ -33,6 +34,9 @@ def main(argv=None) -> int:
                          "C = A^T A, or a batch of --count products of n rows and widths m x k in one launch")
     ap.add_argument("--count", type=int, default=64, help="problems in the batch (--form batched)")
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64", help="storage type of the backward")
+    ap.add_argument("--layout", choices=["row", "col"], default="row",
+                    help="plain form: row-major operands, or column-major ones (A^T, B^T stored row-major, "
+                         "through tsm_gemm_tn_strided_f64)")
     args = ap.parse_args(argv)
 
     from tsm_benchmark_b200 import (BatchedTSMTTSM, fill_uniform, gram, tsmttsm, tsmttsm_backward, tsmttsm_split,
@@ -93,10 +97,17 @@ def main(argv=None) -> int:
         ms = ev0.elapsed_time(ev1) / args.reps
         print(f"{args.form} {args.dtype if args.form == 'backward' else 'f32'} n={args.n} m={args.m} k={args.k}: {ms:.4f} ms/call, {nbytes / (ms * 1e-3) / 1e9:.1f} GB/s")
         return 0
-    A = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
-    B = torch.empty((args.n, args.k), dtype=torch.float64, device=dev)
-    fill_uniform(A, 1, 0)
-    fill_uniform(B, 1, 1)
+    if args.layout == "col":
+        At = torch.empty((args.m, args.n), dtype=torch.float64, device=dev)
+        Bt = torch.empty((args.k, args.n), dtype=torch.float64, device=dev)
+        fill_uniform(At, 1, 0)
+        fill_uniform(Bt, 1, 1)
+        A, B = At.t(), Bt.t()
+    else:
+        A = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
+        B = torch.empty((args.n, args.k), dtype=torch.float64, device=dev)
+        fill_uniform(A, 1, 0)
+        fill_uniform(B, 1, 1)
     vidx = -1
     if args.variant:
         names = {v["name"]: v["index"] for v in variants()}
@@ -114,7 +125,8 @@ def main(argv=None) -> int:
     chk = float((A.sum(1) * B.sum(1)).sum())
     bound = 32 * math.sqrt(args.n) * 2.0**-53 * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B))
     ok = abs(float(C.sum()) - chk) <= bound * math.sqrt(args.m * args.k)
-    print(f"n={args.n} m={args.m} k={args.k} reps={args.reps}: {ms:.4f} ms/call, {gbs:.1f} GB/s, checksum "
+    print(f"{'column-major ' if args.layout == 'col' else ''}n={args.n} m={args.m} k={args.k} reps={args.reps}: "
+          f"{ms:.4f} ms/call, {gbs:.1f} GB/s, checksum "
           f"{'ok' if ok else 'MISMATCH'}")
     return 0 if ok else 1
 
