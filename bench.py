@@ -251,7 +251,8 @@ def forms(dev) -> dict:
     GPU: split precision (n = 2^25, m = k = 32, FP32 storage, column scaled
     normal data), batched (512 problems, one launch under a CUDA graph vs one
     plain launch per problem), the Gram product C = A^T A (vs the
-    two-operand call on a copy of A) and differentiation (n = 2^22,
+    two-operand call on a copy of A), column-major operands (vs the
+    row-major call on the same values) and differentiation (n = 2^22,
     m = k = 16: fused backward vs forward time, FP64 and FP32)."""
     import numpy as np
     import torch
@@ -334,6 +335,28 @@ def forms(dev) -> dict:
         del A, A2
         torch.cuda.empty_cache()
     out["gram"] = rows
+
+    # --- column-major operands (A^T, B^T stored row-major, through
+    #     tsm_gemm_tn_strided_f64) vs the row-major call on the same values
+    rows = []
+    for cm, ck, cn in ((8, 8, 1 << 26), (4, 32, 1 << 25), (32, 32, 1 << 25), (64, 64, 1 << 23)):
+        At = torch.empty((cm, cn), dtype=torch.float64, device=dev)
+        Bt = torch.empty((ck, cn), dtype=torch.float64, device=dev)
+        tsm.fill_uniform(At, 91, 0)
+        tsm.fill_uniform(Bt, 91, 1)
+        Ar, Br = At.t().contiguous(), Bt.t().contiguous()
+        Cc = torch.empty((cm, ck), dtype=torch.float64, device=dev)
+        Cr = torch.empty((cm, ck), dtype=torch.float64, device=dev)
+        ms_c = _time(lambda: tsm.tsmttsm(At.t(), Bt.t(), Cc), 10)
+        ms_r = _time(lambda: tsm.tsmttsm(Ar, Br, Cr), 10)
+        nbytes = 8 * cn * (cm + ck)
+        rows.append({"n": cn, "m": cm, "k": ck, "column_major_ms": round(ms_c, 4), "row_major_ms": round(ms_r, 4),
+                     "column_major_GB/s": round(nbytes / (ms_c * 1e-3) / 1e9, 1),
+                     "row_major_GB/s": round(nbytes / (ms_r * 1e-3) / 1e9, 1),
+                     "max_rel_diff": float((Cc - Cr).abs().max() / Cr.abs().max())})
+        del At, Bt, Ar, Br
+        torch.cuda.empty_cache()
+    out["column_major"] = rows
 
     # --- differentiation: fused backward vs forward
     n, w = 1 << 22, 16

@@ -82,3 +82,38 @@ def test_split_and_backward_write_only_outputs(gpu, oracle_mod):
     dCn = dC.cpu().numpy()
     assert np.allclose(gA.cpu().numpy(), oracle_mod.tsmm(B, dCn.T.copy()), rtol=1e-12, atol=1e-12)
     assert np.allclose(gB.cpu().numpy(), oracle_mod.tsmm(A, dCn), rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("m,k,layout", [(4, 4, "col"), (8, 8, "col"), (1, 64, "col"), (32, 32, "col"),
+                                        (4, 32, "col"), (64, 64, "col"), (5, 7, "mixed"), (64, 64, "mixed")])
+def test_strided_layouts_write_only_c(gpu, oracle_mod, m, k, layout):
+    """Column-major operands (tensor-map SIMT and FP64 tensor-core kernels)
+    and a mixed layout (the strided register-tile kernel)."""
+    from tsm_benchmark_b200 import _capi
+    lib = _capi.load()
+    sh = torch.cuda.current_stream(gpu).cuda_stream
+    n = 50021
+    A, B = oracle_mod.operands(n, m, k, 31 + m + k)
+    At = to_dev(A.T, gpu)  # m x n row-major: A column-major with pitch n
+    Bt = to_dev(B.T, gpu)
+    need = lib.tsm_gemm_tn_workspace_size(n, m, k)
+    ws = torch.full((need + 4096,), 0xA5, dtype=torch.uint8, device=gpu)
+    ws[:need] = 0
+    buf, C = framed(m, k, gpu)
+    if layout == "col":
+        # pitch n + 1 is even for n = 50021: the pipelined kernels
+        Ap = torch.zeros((m, n + 1), dtype=torch.float64, device=gpu)
+        Bp = torch.zeros((k, n + 1), dtype=torch.float64, device=gpu)
+        Ap[:, :n] = At
+        Bp[:, :n] = Bt
+        args = (Ap.data_ptr(), 1, n + 1, Bp.data_ptr(), 1, n + 1)
+    else:
+        Ar = to_dev(A, gpu)
+        args = (Ar.data_ptr(), m, 1, Bt.data_ptr(), 1, n)
+    st = lib.tsm_gemm_tn_strided_f64(sh, n, m, k, *args, C.data_ptr(), C.stride(0), 0, ws.data_ptr(), need)
+    assert st == 0
+    torch.cuda.synchronize()
+    assert_frame(buf, m, k, f"C frame {m}x{k} {layout}")
+    assert bool((ws[need:] == 0xA5).all()), "workspace tail"
+    ref = oracle_mod.naive(A, B)
+    assert np.allclose(C.cpu().numpy(), ref, rtol=1e-12, atol=1e-9 * np.abs(ref).max())
