@@ -65,3 +65,66 @@ def test_shard_rows_balanced():
             assert all(spans[i][1] == spans[i + 1][0] for i in range(world - 1))
             sizes = [b - a for a, b in spans]
             assert max(sizes) - min(sizes) <= 1
+
+
+def _batch_worker(rank: int, world: int, port: int, out_dir: str):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    from tsm_benchmark_b200.distributed import batched_sharded, shard_problems
+    shapes = _batch_shapes()
+    owned = shard_problems([8 * n * (m + k) for n, m, k in shapes], world)[rank]
+    As, Bs = [], []
+    for i in owned:
+        a, b = _batch_operands(i, shapes[i])
+        As.append(a)
+        Bs.append(b)
+    Cs = batched_sharded(As, Bs, shapes, local_fn=lambda xs, ys: [x.T @ y for x, y in zip(xs, ys)])
+    torch.save({"Cs": Cs, "owned": owned}, os.path.join(out_dir, f"batch{rank}.pt"))
+    dist.destroy_process_group()
+
+
+def _batch_shapes():
+    g = torch.Generator().manual_seed(11)
+    ns = torch.randint(1, 3000, (37,), generator=g).tolist()
+    ms = torch.randint(1, 9, (37,), generator=g).tolist()
+    ks = torch.randint(1, 9, (37,), generator=g).tolist()
+    return list(zip(ns, ms, ks))
+
+
+def _batch_operands(i, shape):
+    n, m, k = shape
+    g = torch.Generator().manual_seed(100 + i)
+    return (torch.rand((n, m), generator=g, dtype=torch.float64) * 2 - 1,
+            torch.rand((n, k), generator=g, dtype=torch.float64) * 2 - 1)
+
+
+def test_batched_sharded_by_problem_two_ranks(tmp_path):
+    """Problems of a batch spread over ranks by cost; every rank ends with
+    every C_i, bit for bit the owner's result."""
+    world = 2
+    mp.start_processes(_batch_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    res = [torch.load(tmp_path / f"batch{r}.pt") for r in range(world)]
+    shapes = _batch_shapes()
+    owned = sorted(res[0]["owned"] + res[1]["owned"])
+    assert owned == list(range(len(shapes))), "each problem owned by exactly one rank"
+    for i, shape in enumerate(shapes):
+        a, b = _batch_operands(i, shape)
+        ref = a.T @ b
+        for r in res:
+            assert torch.equal(r["Cs"][i], ref), (i, shape)
+
+
+def test_shard_problems_balanced_and_deterministic():
+    from tsm_benchmark_b200.distributed import shard_problems
+    costs = [5, 1, 9, 3, 3, 7, 2, 8, 8, 1]
+    for world in (1, 2, 3, 4, 16):
+        a = shard_problems(costs, world)
+        assert a == shard_problems(costs, world)
+        assert sorted(i for o in a for i in o) == list(range(len(costs)))
+        loads = [sum(costs[i] for i in o) for o in a]
+        # longest-first greedy: no rank exceeds the lightest by more than the largest single cost
+        assert max(loads) - min(loads) <= max(costs)
+    assert shard_problems([], 3) == [[], [], []]
