@@ -111,6 +111,19 @@ tsm_status tsm_gemm_tn_f32_split(tsm_stream_t stream, int64_t n, int m, int k, c
                                  const float* B, int64_t ldb, double* C, int64_t ldc, int accumulate, void* workspace,
                                  size_t workspace_bytes);
 
+/* The precision form with BF16 parts (kind::f16 tensor-core MMAs, K = 16
+ * rows per instruction): each FP32 value is split into `parts` BF16 values,
+ * h = rn(x) then rn of the remainder -- parts = 2 (hi/lo): |x - h - l| <=
+ * 2^-16 |x|, about 1e-5 relative error on C, ABOVE the 1e-6 of the TF32
+ * form; parts = 3 (hi/mid/lo): <= 2^-24 |x|.  One MMA per 16 rows forms all
+ * parts x parts products, FP32 accumulation per 64 rows, FP64 beyond.  A and
+ * B contiguous (lda = m, ldb = k), 16-byte aligned, m and k multiples of 4
+ * up to 32 (else TSM_ERROR_UNSUPPORTED).  No counterpart in the reference.
+ * Workspace: as tsm_gemm_tn_workspace_size(n, m, k). */
+tsm_status tsm_gemm_tn_f32_split_bf16(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
+                                      const float* B, int64_t ldb, double* C, int64_t ldc, int accumulate, int parts,
+                                      void* workspace, size_t workspace_bytes);
+
 /* Element types of the plain entry points. */
 #define TSM_F64 0
 #define TSM_F32 1

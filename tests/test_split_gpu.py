@@ -78,3 +78,48 @@ def test_split_full_config(gpu):
     assert nw <= TARGET and pe <= TARGET, (nw, pe)
     del A, B
     torch.cuda.empty_cache()
+
+
+# BF16 parts (tsm_gemm_tn_f32_split_bf16).  Per value |x - sum of parts| <=
+# 2^-16 |x| (2 parts) or 2^-24 |x| (3 parts), so each product is off by at most
+# (2 2^-16 + 2^-32) |a b| (2 parts: ~3.05e-5) or ~2^-23 |a b| (3 parts), plus
+# the FP32 accumulation of 64-row tiles.
+BF16_TOL = {2: 4e-5, 3: TARGET}
+BF16_SHAPES = [(4096, 32, 32), (100003, 32, 32), (3, 32, 32), (0, 8, 8), (20000, 32, 4), (1 << 20, 16, 16),
+               (70001, 8, 24), (129, 12, 28), (1, 4, 4), (63, 4, 8), (64, 8, 8), (65, 32, 32), (257, 32, 8)]
+
+
+@pytest.mark.parametrize("parts", [2, 3])
+@pytest.mark.parametrize("n,m,k", BF16_SHAPES)
+def test_split_bf16_parity(gpu, oracle_mod, parts, n, m, k):
+    from tsm_benchmark_b200 import tsmttsm_split, workspace_status
+    A = scaled_normal(n, m, 7 * n + m)
+    B = scaled_normal(n, k, 7 * n + k + 1)
+    C = tsmttsm_split(torch.from_numpy(A).to(gpu), torch.from_numpy(B).to(gpu), kind=f"bf16x{parts}")
+    torch.cuda.synchronize()
+    assert workspace_status(gpu) == 0
+    got = C.cpu().numpy()
+    ref = oracle_mod.naive(A, B)
+    if n == 0:
+        assert np.all(got == 0)
+        return
+    nw, pe = errors(ref, got, A, B)
+    assert nw <= BF16_TOL[parts] and pe <= BF16_TOL[parts], (nw, pe)
+
+
+def test_split_bf16_deterministic_accumulate_and_limits(gpu):
+    from tsm_benchmark_b200 import tsmttsm_split
+    A = torch.from_numpy(scaled_normal(50000, 32, 3)).to(gpu)
+    B = torch.from_numpy(scaled_normal(50000, 32, 4)).to(gpu)
+    for kind in ("bf16x2", "bf16x3"):
+        first = tsmttsm_split(A, B, kind=kind).clone()
+        for _ in range(3):
+            assert torch.equal(tsmttsm_split(A, B, kind=kind), first)
+        C = first.clone()
+        tsmttsm_split(A, B, C, accumulate=True, kind=kind)
+        assert torch.allclose(C, 2 * first, rtol=1e-15, atol=0)
+    # widths that are not multiples of 4 are not taken (the TF32 kind takes them)
+    from tsm_benchmark_b200._capi import TsmError
+    A5 = torch.zeros((100, 5), dtype=torch.float32, device=gpu)
+    with pytest.raises(TsmError):
+        tsmttsm_split(A5, A5, kind="bf16x3")

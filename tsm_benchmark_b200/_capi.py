@@ -84,6 +84,8 @@ SIGNATURES = {
                                 c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_f32_variant": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int, c_void_p, c_size_t, c_int]),
+    "tsm_gemm_tn_f32_split_bf16": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                           c_void_p, c_int64, c_int, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_f32_split": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                       c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_default_variant": (c_int, [c_int, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64]),

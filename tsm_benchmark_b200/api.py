@@ -286,11 +286,19 @@ def tsmttsm_backward(A: torch.Tensor, B: torch.Tensor, dC: torch.Tensor, *, need
     return dA, dB
 
 
+_SPLIT_KINDS = {"tf32": 0, "bf16x2": 2, "bf16x3": 3}
+
+
 def tsmttsm_split(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, accumulate: bool = False,
-                  stream: torch.cuda.Stream | None = None) -> torch.Tensor:
-    """C (float64) = A^T B for float32 A, B (m, k <= 32) on the tensor cores:
-    TF32 hi/lo split, FP32 accumulation per 128 rows, FP64 sums
-    (``tsm_gemm_tn_f32_split``)."""
+                  kind: str = "tf32", stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """C (float64) = A^T B for float32 A, B (m, k <= 32) on the tensor cores,
+    FP32 accumulation per tile, FP64 sums.  ``kind``: "tf32" -- TF32 hi/lo
+    parts (``tsm_gemm_tn_f32_split``, error <= 1e-6); "bf16x2" -- BF16
+    hi/lo (``tsm_gemm_tn_f32_split_bf16`` with 2 parts, about 1e-5);
+    "bf16x3" -- BF16 hi/mid/lo (3 parts).  The BF16 kinds need m and k
+    multiples of 4."""
+    if kind not in _SPLIT_KINDS:
+        raise ValueError(f"kind must be one of {sorted(_SPLIT_KINDS)}, got {kind!r}")
     _check_operand(A, "A", torch.float32)
     _check_operand(B, "B", torch.float32)
     n, m = A.shape
@@ -308,7 +316,13 @@ def tsmttsm_split(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = Non
         sh = _stream_handle(A.device, stream)
         need = lib.tsm_gemm_tn_workspace_size(n, m, k)
         ws = workspace(A.device, need, sh)
-        st = lib.tsm_gemm_tn_f32_split(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
-                                       _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel())
-        _capi.check(st, "tsm_gemm_tn_f32_split")
+        if kind == "tf32":
+            st = lib.tsm_gemm_tn_f32_split(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
+                                           _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel())
+            _capi.check(st, "tsm_gemm_tn_f32_split")
+        else:
+            st = lib.tsm_gemm_tn_f32_split_bf16(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B),
+                                                C.data_ptr(), _ld(C), 1 if accumulate else 0, _SPLIT_KINDS[kind],
+                                                ws.data_ptr(), ws.numel())
+            _capi.check(st, "tsm_gemm_tn_f32_split_bf16")
     return C

@@ -1,7 +1,8 @@
-// tsm_split.cu -- C ABI of the precision form (FP32 storage, TF32 hi/lo
-// split on tcgen05 tensor cores, FP64 reductions).  Kernels: tsm_split_tma.cuh
+// tsm_split.cu -- C ABI of the precision form (FP32 storage, hi/lo parts on
+// the tcgen05 tensor cores, FP64 reductions).  TF32 parts: tsm_split_tma.cuh
 // (widths that are multiples of 4: 2-D TMA straight into the MMA layout) and
-// tsm_split.cuh (any width: 1-D bulk copies and a converter pass).
+// tsm_split.cuh (any width: 1-D bulk copies and a converter pass).  BF16
+// parts (two or three): tsm_split_bf16.cuh.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -14,6 +15,7 @@
 #include "../../include/tsm.h"
 #include "tsm_errors.h"
 #include "tsm_split.cuh"
+#include "tsm_split_bf16.cuh"
 #include "tsm_split_tma.cuh"
 #include "tsm_tmap.h"
 
@@ -131,5 +133,77 @@ extern "C" tsm_status tsm_gemm_tn_f32_split(tsm_stream_t stream, int64_t n, int 
   e = cudaLaunchKernel(reinterpret_cast<const void*>(&tsm_tn_split_tf32_kernel), dim3(static_cast<unsigned>(grid)),
                        dim3(split::kThreads), args, split::kSmemBytes, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return split_fail(e, "cudaLaunchKernel(split)");
+  return TSM_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// BF16 parts (tsm_split_bf16.cuh): 2 (hi/lo) or 3 (hi/mid/lo) parts.
+namespace tsm {
+namespace {
+bool g_split16_attr[64][2] = {};
+}  // namespace
+}  // namespace tsm
+
+extern "C" tsm_status tsm_gemm_tn_f32_split_bf16(tsm_stream_t stream, int64_t n, int m, int k, const float* A,
+                                                 int64_t lda, const float* B, int64_t ldb, double* C, int64_t ldc,
+                                                 int accumulate, int parts, void* workspace,
+                                                 size_t workspace_bytes) {
+  if (n < 0 || m < 1 || k < 1 || m > 32 || k > 32 || ldc < k || C == nullptr) return TSM_ERROR_INVALID_VALUE;
+  if (parts != 2 && parts != 3) return TSM_ERROR_INVALID_VALUE;
+  if (n > 0 && (A == nullptr || B == nullptr)) return TSM_ERROR_INVALID_VALUE;
+  // Tensor maps: 16-byte row pitches and bases, 32-bit row coordinates.
+  if (lda != m || ldb != k || m % 4 != 0 || k % 4 != 0 || !aligned16(A) || !aligned16(B) ||
+      n > static_cast<int64_t>(INT_MAX) - split16::kRows)
+    return TSM_ERROR_UNSUPPORTED;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return split_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return TSM_ERROR_UNSUPPORTED;
+  const void* fn = parts == 2 ? reinterpret_cast<const void*>(&tsm_tn_split_bf16_kernel<2>)
+                              : reinterpret_cast<const void*>(&tsm_tn_split_bf16_kernel<3>);
+  const size_t smem = parts == 2 ? split16::Shape<2>::SMEM_BYTES : split16::Shape<3>::SMEM_BYTES;
+  {
+    std::lock_guard<std::mutex> lk(g_split_mu);
+    if (g_split_sms[dev] == 0) {
+      e = cudaDeviceGetAttribute(&g_split_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return split_fail(e, "cudaDeviceGetAttribute");
+    }
+    if (!g_split16_attr[dev][parts - 2]) {
+      e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e != cudaSuccess) return split_fail(e, "cudaFuncSetAttribute(split bf16)");
+      g_split16_attr[dev][parts - 2] = true;
+    }
+  }
+  const int sms = g_split_sms[dev];
+  const size_t need = 256 + static_cast<size_t>(sms) * 4 * m * k * sizeof(double);
+  if (workspace == nullptr || workspace_bytes < need || !aligned16(workspace)) return TSM_ERROR_WORKSPACE;
+  SplitTmaArgs a{};
+  SplitArgs& p = a.p;
+  p.A = A;
+  p.B = B;
+  p.C = C;
+  p.n = n;
+  p.m = m;
+  p.k = k;
+  p.ldc = ldc;
+  p.accumulate = accumulate ? 1 : 0;
+  unsigned char* base = static_cast<unsigned char*>(workspace);
+  p.counter = reinterpret_cast<unsigned*>(base);
+  p.error = reinterpret_cast<unsigned*>(base) + 1;
+  p.partials = reinterpret_cast<double*>(base + 256);
+  p.rows_main = n;  // the tensor maps zero-fill past row n
+  p.num_chunks = (n + split16::kRows - 1) / split16::kRows;
+  if (n > 0) {  // n = 0: no chunks, the maps are never read
+    if (!encode_rowmajor_map(&a.ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, n, m, lda, 32, split16::kRows,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, &last_error()) ||
+        !encode_rowmajor_map(&a.tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, B, n, k, ldb, 32, split16::kRows,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, &last_error()))
+      return TSM_ERROR_CUDA;
+  }
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(p.num_chunks, sms));
+  void* args[] = {&a};
+  e = cudaLaunchKernel(fn, dim3(static_cast<unsigned>(grid)), dim3(split16::kThreads), args, smem,
+                       static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return split_fail(e, "cudaLaunchKernel(split bf16)");
   return TSM_SUCCESS;
 }

@@ -92,6 +92,8 @@ __device__ __forceinline__ uint32_t op_offset(int r, int c) {
 // i and 32 + i -- the hi and lo parts of A's column i -- added) into the
 // workspace, and the last CTA's fixed-order sum over CTAs (plus the rows
 // [rows_main, n) the pipeline left) into C.
+__device__ __forceinline__ void split_finish_ctas(const SplitArgs& p, int t, int nthreads, unsigned* s_is_last);
+
 __device__ __forceinline__ void split_finish(const SplitArgs& p, const double (&acc)[32], double* red, int t,
                                              int nthreads, int epi0, unsigned* s_is_last) {
   const int warp = t >> 5, lane = t & 31;
@@ -111,6 +113,15 @@ __device__ __forceinline__ void split_finish(const SplitArgs& p, const double (&
     const int lo_slot = (2 + (i >> 4)) * 16 + (i & 15);
     mine[e] = red[hi_slot * 32 + j] + red[lo_slot * 32 + j];
   }
+  split_finish_ctas(p, t, nthreads, s_is_last);
+}
+
+// The CTA's partial is in the workspace (slot blockIdx.x): count the CTA in,
+// and the last one sums the CTA partials in CTA order (plus the rows
+// [rows_main, n) the pipeline left) into C.
+__device__ __forceinline__ void split_finish_ctas(const SplitArgs& p, int t, int nthreads, unsigned* s_is_last) {
+  const int m = p.m, k = p.k;
+  const int mk = m * k;
   __threadfence();
   __syncthreads();
   if (t == 0) {

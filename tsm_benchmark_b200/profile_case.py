@@ -34,6 +34,8 @@ def main(argv=None) -> int:
                          "C = A^T A, or a batch of --count products of n rows and widths m x k in one launch")
     ap.add_argument("--count", type=int, default=64, help="problems in the batch (--form batched)")
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64", help="storage type of the backward")
+    ap.add_argument("--split-kind", choices=["tf32", "bf16x2", "bf16x3"], default="tf32",
+                    help="parts of the split form (--form split)")
     ap.add_argument("--layout", choices=["row", "col"], default="row",
                     help="plain form: row-major operands, or column-major ones (A^T, B^T stored row-major, "
                          "through tsm_gemm_tn_strided_f64)")
@@ -78,7 +80,7 @@ def main(argv=None) -> int:
         fill_uniform(B, 1, 1)
         if args.form == "split":
             A, B = A.float(), B.float()
-            run = lambda: tsmttsm_split(A, B)  # noqa: E731
+            run = lambda: tsmttsm_split(A, B, kind=args.split_kind)  # noqa: E731
             nbytes = 4 * args.n * (args.m + args.k)
         else:
             dt = torch.float64 if args.dtype == "f64" else torch.float32
@@ -95,7 +97,7 @@ def main(argv=None) -> int:
         ev1.record()
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1) / args.reps
-        print(f"{args.form} {args.dtype if args.form == 'backward' else 'f32'} n={args.n} m={args.m} k={args.k}: {ms:.4f} ms/call, {nbytes / (ms * 1e-3) / 1e9:.1f} GB/s")
+        print(f"{args.form} {args.dtype if args.form == 'backward' else args.split_kind} n={args.n} m={args.m} k={args.k}: {ms:.4f} ms/call, {nbytes / (ms * 1e-3) / 1e9:.1f} GB/s")
         return 0
     if args.layout == "col":
         At = torch.empty((args.m, args.n), dtype=torch.float64, device=dev)
