@@ -25,14 +25,14 @@
 //
 // Pipeline, one persistent CTA per SM (16 warps):
 //   warp 0       TMA producer: 64-row boxes of raw FP32 A and B (tensor maps,
-//                32 columns, zero fill past m, k and n) into an 8-deep raw ring
+//                32 columns, zero fill past m, k and n) into a raw ring
 //   warps 2-9    converters: lane c takes column c of 8 rows of A or B, splits
 //                the 8 values into PARTS BF16 parts and writes each part as
 //                one 16-byte chunk (8 consecutive K values) of operand row
 //                32 p + c -- a warp's 8 chunks per 8-lane phase land in 8
 //                different bank groups (chunk rg ^ (c mod 8))
 //   warps 1, 14, 15  MMA issuers: chunk it goes to issuer it mod 3, which
-//                owns operand stage it mod 3 and TMEM accumulator it mod 3
+//                owns operand stages it mod 6 and TMEM accumulator it mod 3
 //                (issuing from one thread was the bottleneck of the TF32 form)
 //                and accumulates kFlush = 2 of its chunks before a drain
 //   warps 10-13  epilogue: warp w reads TMEM lanes 32 w .. +31, i.e. A's part
@@ -59,9 +59,9 @@ namespace tsm {
 namespace split16 {
 
 constexpr int kRows = 64;                      // rows per chunk: 4 MMAs of K = 16
-constexpr int kRawStages = 8;
 constexpr int kIssuers = 3;
-constexpr int kOpStages = kIssuers;            // one operand stage per issuer
+constexpr int kOpStages = 2 * kIssuers;        // two operand stages per issuer: converters run a round ahead
+static_assert(kOpStages % kIssuers == 0, "an operand stage belongs to one issuer");
 constexpr int kFlush = 2;                      // an issuer's chunks per accumulator drain (128 rows)
 constexpr int kRawTile = kRows * 32 * 4;       // one operand: 64 rows x 32 floats (8 KB)
 constexpr int kRawStageBytes = 2 * kRawTile;   // A, B
@@ -81,10 +81,13 @@ struct Shape {
   static constexpr int N = 32 * PARTS;
   static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
                                     (static_cast<uint32_t>(128 >> 4) << 24);  // F32 D, BF16 A/B, K-major
+  // Raw ring depth: what shared memory leaves (the pipeline is not bound by
+  // HBM: a timing copy with no copies at all ran within 2 %).
+  static constexpr int RAW_STAGES = PARTS == 2 ? 8 : 4;
   static constexpr size_t OP_OFFSET = 0;
   static constexpr size_t RAW_OFFSET = OP_OFFSET + size_t(kOpStages) * OP_STAGE;
-  static constexpr size_t BAR_OFFSET = RAW_OFFSET + size_t(kRawStages) * kRawStageBytes;
-  static constexpr int NUM_BARS = 2 * kRawStages + 2 * kOpStages + 2 * kIssuers;
+  static constexpr size_t BAR_OFFSET = RAW_OFFSET + size_t(RAW_STAGES) * kRawStageBytes;
+  static constexpr int NUM_BARS = 2 * RAW_STAGES + 2 * kOpStages + 2 * kIssuers;
   static constexpr size_t SMEM_BYTES = BAR_OFFSET + NUM_BARS * 8 + 32 + 1024;  // + alignment slack
   static_assert(SMEM_BYTES <= 232448, "dynamic shared memory limit of sm_100a");
   static_assert(OP_STAGE % 1024 == 0 && RAW_OFFSET % 1024 == 0, "1024-byte aligned swizzle atoms");
@@ -111,8 +114,8 @@ __global__ void __launch_bounds__(split16::kThreads, 1)
   unsigned char* smem = smem_raw + ((1024u - (dev::smem_u32(smem_raw) & 1023u)) & 1023u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::BAR_OFFSET);
   uint64_t* raw_full = bars;                      // raw stage landed (TMA transaction count)
-  uint64_t* raw_empty = raw_full + kRawStages;    // raw stage read (converter warps)
-  uint64_t* op_full = raw_empty + kRawStages;     // operand stage written (converter warps)
+  uint64_t* raw_empty = raw_full + S::RAW_STAGES;    // raw stage read (converter warps)
+  uint64_t* op_full = raw_empty + S::RAW_STAGES;     // operand stage written (converter warps)
   uint64_t* op_empty = op_full + kOpStages;       // operand stage's MMAs completed (commit)
   uint64_t* d_full = op_empty + kOpStages;        // accumulator b complete (commit)
   uint64_t* d_empty = d_full + kIssuers;          // accumulator b drained (epilogue warps)
@@ -125,7 +128,7 @@ __global__ void __launch_bounds__(split16::kThreads, 1)
   const int64_t G = gridDim.x;
 
   if (t == 0) {
-    for (int s = 0; s < kRawStages; ++s) {
+    for (int s = 0; s < S::RAW_STAGES; ++s) {
       dev::mbar_init(&raw_full[s], 1);
       dev::mbar_init(&raw_empty[s], kConvWarps);
     }
@@ -164,11 +167,11 @@ __global__ void __launch_bounds__(split16::kThreads, 1)
     }
     const uint64_t policy = dev::policy_evict_first();
     for (int64_t it = 0; it < nchunks_mine; ++it) {
-      const int s = static_cast<int>(it % kRawStages);
+      const int s = static_cast<int>(it % S::RAW_STAGES);
       bool ok = true;
       if (lane == 0) {
-        if (it >= kRawStages)
-          ok = dev::mbar_wait(&raw_empty[s], static_cast<uint32_t>(((it / kRawStages) - 1) & 1), abort);
+        if (it >= S::RAW_STAGES)
+          ok = dev::mbar_wait(&raw_empty[s], static_cast<uint32_t>(((it / S::RAW_STAGES) - 1) & 1), abort);
         if (ok) {
           unsigned char* st = smem + S::RAW_OFFSET + s * kRawStageBytes;
           const int y = static_cast<int>((blockIdx.x + it * G) * kRows);
@@ -224,9 +227,9 @@ __global__ void __launch_bounds__(split16::kThreads, 1)
     // A and of B; lane = column.
     const int cw = warp - 2;
     for (int64_t it = 0; it < nchunks_mine; ++it) {
-      const int s = static_cast<int>(it % kRawStages);
+      const int s = static_cast<int>(it % S::RAW_STAGES);
       const int o = static_cast<int>(it % kOpStages);
-      bool ok = dev::mbar_wait(&raw_full[s], static_cast<uint32_t>((it / kRawStages) & 1), abort);
+      bool ok = dev::mbar_wait(&raw_full[s], static_cast<uint32_t>((it / S::RAW_STAGES) & 1), abort);
       if (ok && it >= kOpStages)
         ok = dev::mbar_wait(&op_empty[o], static_cast<uint32_t>(((it / kOpStages) - 1) & 1), abort);
       if (!ok) {
@@ -319,8 +322,8 @@ __global__ void __launch_bounds__(split16::kThreads, 1)
     // is only recorded.
     volatile int no_abort = 0;
     if (warp == 0) {
-      for (int64_t it = nchunks_mine > kRawStages ? nchunks_mine - kRawStages : 0; it < nchunks_mine; ++it)
-        if (!dev::mbar_wait(&raw_full[it % kRawStages], static_cast<uint32_t>((it / kRawStages) & 1), &no_abort))
+      for (int64_t it = nchunks_mine > S::RAW_STAGES ? nchunks_mine - S::RAW_STAGES : 0; it < nchunks_mine; ++it)
+        if (!dev::mbar_wait(&raw_full[it % S::RAW_STAGES], static_cast<uint32_t>((it / S::RAW_STAGES) & 1), &no_abort))
           break;
     } else if (warp == 1) {
       for (int b = 0; b < kIssuers; ++b) {
