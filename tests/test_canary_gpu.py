@@ -67,6 +67,13 @@ def test_split_and_backward_write_only_outputs(gpu, oracle_mod):
                                      0, ws.data_ptr(), need) == 0
     torch.cuda.synchronize()
     assert_frame(buf, m, k, "split C frame")
+    for parts in (2, 3):  # BF16 parts
+        buf, C = framed(m, k, gpu)
+        assert lib.tsm_gemm_tn_f32_split_bf16(sh, n, m, k, A32.data_ptr(), m, B32.data_ptr(), k, C.data_ptr(),
+                                              C.stride(0), 0, parts, ws.data_ptr(), need) == 0
+        torch.cuda.synchronize()
+        assert_frame(buf, m, k, f"split bf16 x{parts} C frame")
+        assert bool((ws[need:] == 0xA5).all()), "workspace tail"
     # fused backward: dA (n x m) and dB (n x k) in frames
     dC = to_dev(np.random.default_rng(1).standard_normal((m, k)), gpu)
     dA_in, dB_in = to_dev(A, gpu), to_dev(B, gpu)
