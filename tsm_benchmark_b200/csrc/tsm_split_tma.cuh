@@ -24,15 +24,17 @@
 // stage to its lo stage as the leading byte offset (LBO) between the hi and
 // lo atoms of an operand.
 //
-// Warp roles (16 warps): 0 producer, 1 TMEM owner + MMA issuer of chunks
-// 0, 3, 6 .., 14 and 15 MMA issuers of chunks 1, 4 .. and 2, 5 .. (issuing
-// tcgen05.mma from one thread was a measured bottleneck: 2^25 x 32 x 32 took
-// 1.79 ms with one issuer, 1.56 with two, 1.53 with three; each issuer owns
-// one lo stage and one TMEM accumulator, so they share no barrier phase),
-// 2-9 converters, 10-13 epilogue (TMEM -> FP64 sums).  A fourth issuer (17
-// warps, three hi stages) drops the register cap to 96 and spills.  All
-// waits are bounded (dev::mbar_wait); on a timeout the CTA records the
-// error, drains its copies and MMAs (bounded) and frees its TMEM.
+// Warp roles (16 warps): 0 producer, 1-3 MMA issuers of chunks 0, 3, 6 ..,
+// 1, 4 .. and 2, 5 .. (warp 1 also owns TMEM; issuing tcgen05.mma from one
+// thread was a measured bottleneck: 2^25 x 32 x 32 took 1.79 ms with one
+// issuer, 1.56 with two, 1.53 with three; each issuer owns one lo stage and
+// one TMEM accumulator, so they share no barrier phase), 4-11 converters,
+// 12-15 epilogue (TMEM -> FP64 sums).  A fourth issuer does not pay: with 17
+// warps the register cap (96) spills the epilogue sums, and with the
+// converters halved to make room (13 warps) the form ran 1.91 ms,
+// converter-bound.  All waits are bounded (dev::mbar_wait); on a timeout the
+// CTA records the error, drains its copies and MMAs (bounded) and frees its
+// TMEM.
 #pragma once
 
 #include <cuda.h>
@@ -57,14 +59,17 @@ constexpr int kRows = 128;                   // rows per chunk (16 MMAs of K = 8
 // kIssuers warps issue the MMAs (chunk it goes to issuer it % kIssuers);
 // each owns one lo stage and one TMEM accumulator.
 constexpr int kIssuers = 3;
-constexpr int kHiStages = kIssuers == 2 ? 5 : 4;
+constexpr int kHiStages = kIssuers == 2 ? 5 : kIssuers == 3 ? 4 : 3;
 constexpr int kLoStages = kIssuers;
 constexpr int kTileBytes = kRows * 128;      // one operand part: 32 floats x 128 rows
 constexpr int kStageBytes = 2 * kTileBytes;  // A part, B part
 constexpr int kLoRing = kHiStages * kStageBytes;  // offset of the lo ring
 constexpr int kConvWarps = 8;
-constexpr int kEpiWarp0 = 10;
-constexpr int kWarps = 13 + kIssuers;  // issuers: warp 1, then warps 14 ..
+constexpr int kConvWarp0 = 1 + kIssuers;           // warps: 0 producer, 1 .. kIssuers issuers,
+constexpr int kEpiWarp0 = kConvWarp0 + kConvWarps;  // then converters, then 4 epilogue warps
+constexpr int kWarps = kEpiWarp0 + 4;
+constexpr int kConvJobs = 2 * kTileBytes / 16 / (32 * kConvWarps);  // 16-byte vectors per converter thread
+static_assert(kConvJobs * 32 * kConvWarps * 16 == 2 * kTileBytes, "converters cover the stage exactly");
 constexpr int kThreads = kWarps * 32;
 constexpr int kTmemCols = kIssuers * 64 <= 128 ? 128 : 256;  // one 64-column accumulator per issuer
 constexpr uint32_t kIdesc = dev::umma_idesc_tf32(64, 64, true, true);
@@ -74,7 +79,7 @@ constexpr size_t kSmemBytes = kBarOffset + kNumBars * 8 + 32 + 1024;  // + align
 static_assert(kTileBytes % 1024 == 0, "tiles keep the 1024-byte alignment of the swizzle atoms");
 static_assert((kLoRing + (kLoStages - 1) * kStageBytes) / 16 < (1 << 14), "LBO must fit the descriptor field");
 static_assert(kSmemBytes <= 232448, "dynamic shared memory limit of sm_100a");
-static_assert(kIssuers == 2 || kIssuers == 3, "four issuers (17 warps) spill the epilogue sums");
+static_assert(kWarps <= 16, "17 warps cap registers at 96 a thread and spill the epilogue sums");
 
 // lo part of x: x - trunc_tf32(x) (exact) rounded to nearest TF32, ties away
 // from zero (add half a TF32 unit to the magnitude bits, clear 13 bits).
@@ -167,11 +172,11 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
     }
-  } else if (warp == 1 || warp >= 14) {
+  } else if (warp <= kIssuers) {
     // ---------------- MMA issuers (lane 0): issuer r (warp 1, then 14 ..)
     // takes the chunks it = r mod kIssuers; the warp stays converged.
     const uint32_t base = dev::smem_u32(smem);
-    const int64_t first = warp == 1 ? 0 : warp - 13;
+    const int64_t first = warp - 1;
     for (int64_t it = first; it < nchunks_mine; it += kIssuers) {
       const int s = static_cast<int>(it % kHiStages);
       const int o = static_cast<int>(it % kLoStages);
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
     }
   } else if (warp < kEpiWarp0) {
     // ---------------- converters: lo parts, elementwise at the hi offsets
-    const int ct = t - 64;  // 0 .. 255
+    const int ct = t - 32 * kConvWarp0;
     for (int64_t it = 0; it < nchunks_mine; ++it) {
       const int s = static_cast<int>(it % kHiStages);
       const int o = static_cast<int>(it % kLoStages);
@@ -221,14 +226,14 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       uint4* lo = reinterpret_cast<uint4*>(smem + kLoRing + o * kStageBytes);
       // A_hi and B_hi: 2 x 16 KB = 2048 16-byte vectors over 256 threads.
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const uint4 v = hi[ct + q * 256];
+      for (int q = 0; q < kConvJobs; ++q) {
+        const uint4 v = hi[ct + q * 32 * kConvWarps];
         uint4 w;
         w.x = lo_part(v.x);
         w.y = lo_part(v.y);
         w.z = lo_part(v.z);
         w.w = lo_part(v.w);
-        lo[ct + q * 256] = w;
+        lo[ct + q * 32 * kConvWarps] = w;
       }
       dev::fence_proxy_async_smem();  // make the lo tiles visible to the tensor core
       __syncwarp();
