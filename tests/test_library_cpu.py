@@ -74,3 +74,43 @@ def test_python_layer_rejects_cpu_tensors():
     A = torch.zeros((10, 4), dtype=torch.float64)
     with pytest.raises(ValueError):
         tsmttsm(A, A)
+
+
+def test_c_abi_rejects_bad_arguments_before_any_cuda_call():
+    """Argument checks that return before the first CUDA runtime call, so they
+    run without a GPU: shapes, strides, part counts, pitches, alignment and
+    the 32-bit row limit of the tensor-map kernels.  The fake device
+    addresses are never dereferenced."""
+    import ctypes
+    from tsm_benchmark_b200 import _capi
+    lib = _capi.load()
+    INVALID, WORKSPACE, UNSUPPORTED = 1, 2, 4
+    P = ctypes.c_void_p(1 << 20)          # 16-byte aligned, never touched
+    Q = ctypes.c_void_p((1 << 20) + 8)    # 8 bytes off a 16-byte boundary
+    big = (1 << 31) - 10                  # past the tensor maps' 32-bit row coordinates
+    # plain FP64: widths, leading dimensions, null C
+    assert lib.tsm_gemm_tn_f64(None, 10, 0, 4, P, 4, P, 4, P, 4, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_f64(None, 10, 65, 4, P, 65, P, 4, P, 4, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_f64(None, 10, 8, 8, P, 7, P, 8, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_f64(None, 10, 8, 8, P, 8, P, 8, None, 8, 0, P, 1 << 20) == INVALID
+    # general strides: every stride >= 1, widths <= 64, C present, operands when n > 0
+    for strides in ((0, 1, 1, 8), (1, 0, 1, 8), (8, 1, -1, 1), (8, 1, 1, 0)):
+        assert lib.tsm_gemm_tn_strided_f64(None, 10, 8, 8, P, strides[0], strides[1], P, strides[2], strides[3],
+                                           P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_strided_f64(None, 10, 8, 80, P, 1, 10, P, 1, 10, P, 80, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_strided_f64(None, 10, 8, 8, None, 1, 10, P, 1, 10, P, 8, 0, P, 1 << 20) == INVALID
+    # TF32 split: widths <= 32, contiguous 16-byte aligned operands
+    assert lib.tsm_gemm_tn_f32_split(None, 10, 33, 8, P, 33, P, 8, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_f32_split(None, 10, 8, 8, P, 12, P, 8, P, 8, 0, P, 1 << 20) == UNSUPPORTED
+    assert lib.tsm_gemm_tn_f32_split(None, 10, 8, 8, Q, 8, P, 8, P, 8, 0, P, 1 << 20) == UNSUPPORTED
+    # BF16 split: 2 or 3 parts, widths multiples of 4, contiguous, aligned, rows below the tensor-map limit
+    for parts in (0, 1, 4):
+        assert lib.tsm_gemm_tn_f32_split_bf16(None, 10, 8, 8, P, 8, P, 8, P, 8, 0, parts, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_f32_split_bf16(None, 10, 5, 8, P, 5, P, 8, P, 8, 0, 3, P, 1 << 20) == UNSUPPORTED
+    assert lib.tsm_gemm_tn_f32_split_bf16(None, 10, 8, 8, P, 16, P, 8, P, 8, 0, 3, P, 1 << 20) == UNSUPPORTED
+    assert lib.tsm_gemm_tn_f32_split_bf16(None, 10, 8, 8, Q, 8, P, 8, P, 8, 0, 3, P, 1 << 20) == UNSUPPORTED
+    assert lib.tsm_gemm_tn_f32_split_bf16(None, big, 8, 8, P, 8, P, 8, P, 8, 0, 2, P, 1 << 20) == UNSUPPORTED
+    # self-test and fill: workspace and count checks
+    assert lib.tsm_selftest_wait_timeout(None, None, 0, 1000) == WORKSPACE
+    assert lib.tsm_fill_uniform_f64(None, P, -1, 1, 0) == INVALID
+    assert lib.tsm_fill_uniform_f64(None, P, 0, 1, 0) == 0
