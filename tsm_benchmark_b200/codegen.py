@@ -373,6 +373,12 @@ def default_variants() -> list:
     # tensor cores for the DMMA widths, SIMT register tiles below 16.
     for w in DMMA_WIDTHS:
         out.append(DmmaVariant(w, w, gram=True))
+    # SIMT Gram kernels, 3 stages of ~64 KB first (the default takes the first
+    # applicable Gram variant; against 6 stages of ~32 KB they streamed A 3-11 %
+    # faster at n = 2^26), the 6-stage ones after them.
+    for w in (1, 2, 4, 8):
+        g = BulkVariant(w, w, default_tile(w), default_tile(w), gram=True)
+        out.append(dataclasses.replace(g, stages=3, rows=2 * g.resolved().rows))
     for w in (1, 2, 4, 8):
         out.append(BulkVariant(w, w, default_tile(w), default_tile(w), gram=True))
     return out

@@ -45,8 +45,9 @@ const Variant kGenPart0[] = {
     TSM_DIRECT_VARIANT("directf32_16x32_t8x8_th256_cap", float, 16, 32, 8, 8, 256, false),
     TSM_DIRECT_VARIANT("directf32_32x64_t8x8_th256_cap", float, 32, 64, 8, 8, 256, false),
     TSM_GRAM_DMMA_VARIANT("dmma_16x16_gram_w8_s4_r256", 16, 8, 4, 256),
+    TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r4096_u1_gram", double, 1, 1, 1, 1, 8, 6, 4096, 1, true, true),
 };
 extern const int kGenPart0Count;
-const int kGenPart0Count = 38;
+const int kGenPart0Count = 39;
 
 }  // namespace tsm

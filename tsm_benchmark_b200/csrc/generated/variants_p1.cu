@@ -45,8 +45,9 @@ const Variant kGenPart1[] = {
     TSM_DIRECT_VARIANT("directf32_16x64_t8x8_th256_cap", float, 16, 64, 8, 8, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x1_t8x1_th256_cap", float, 64, 1, 8, 1, 256, false),
     TSM_GRAM_DMMA_VARIANT("dmma_32x32_gram_w8_s3_r256", 32, 8, 3, 256),
+    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r2048_u1_gram", double, 2, 2, 2, 2, 8, 6, 2048, 1, true, true),
 };
 extern const int kGenPart1Count;
-const int kGenPart1Count = 38;
+const int kGenPart1Count = 39;
 
 }  // namespace tsm

@@ -45,8 +45,9 @@ const Variant kGenPart2[] = {
     TSM_DIRECT_VARIANT("directf32_32x1_t8x1_th256_cap", float, 32, 1, 8, 1, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x2_t8x2_th256_cap", float, 64, 2, 8, 2, 256, false),
     TSM_GRAM_DMMA_VARIANT("dmma_48x48_gram_w8_s3_r160", 48, 8, 3, 160),
+    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r1024_u1_gram", double, 4, 4, 4, 4, 8, 6, 1024, 1, true, true),
 };
 extern const int kGenPart2Count;
-const int kGenPart2Count = 38;
+const int kGenPart2Count = 39;
 
 }  // namespace tsm

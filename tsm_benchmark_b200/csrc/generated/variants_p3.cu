@@ -45,8 +45,9 @@ const Variant kGenPart3[] = {
     TSM_DIRECT_VARIANT("directf32_32x2_t8x2_th256_cap", float, 32, 2, 8, 2, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x4_t8x4_th256_cap", float, 64, 4, 8, 4, 256, false),
     TSM_GRAM_DMMA_VARIANT("dmma_64x64_gram_w8_s3_r128", 64, 8, 3, 128),
+    TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s6_r512_u1_gram", double, 8, 8, 4, 4, 8, 6, 512, 1, true, true),
 };
 extern const int kGenPart3Count;
-const int kGenPart3Count = 38;
+const int kGenPart3Count = 39;
 
 }  // namespace tsm

@@ -44,7 +44,7 @@ const Variant kGenPart4[] = {
     TSM_DIRECT_VARIANT("directf32_16x2_t8x2_th256_cap", float, 16, 2, 8, 2, 256, false),
     TSM_DIRECT_VARIANT("directf32_32x4_t8x4_th256_cap", float, 32, 4, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x8_t8x4_th256_cap", float, 64, 8, 8, 4, 256, false),
-    TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r4096_u1_gram", double, 1, 1, 1, 1, 8, 6, 4096, 1, true, true),
+    TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s3_r8192_u1_gram", double, 1, 1, 1, 1, 8, 3, 8192, 1, true, true),
 };
 extern const int kGenPart4Count;
 const int kGenPart4Count = 38;

@@ -44,7 +44,7 @@ const Variant kGenPart5[] = {
     TSM_DIRECT_VARIANT("directf32_16x4_t8x4_th256_cap", float, 16, 4, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("directf32_32x8_t8x4_th256_cap", float, 32, 8, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x16_t8x8_th256_cap", float, 64, 16, 8, 8, 256, false),
-    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r2048_u1_gram", double, 2, 2, 2, 2, 8, 6, 2048, 1, true, true),
+    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s3_r4096_u1_gram", double, 2, 2, 2, 2, 8, 3, 4096, 1, true, true),
 };
 extern const int kGenPart5Count;
 const int kGenPart5Count = 38;

@@ -44,7 +44,7 @@ const Variant kGenPart6[] = {
     TSM_DIRECT_VARIANT("directf32_16x8_t8x4_th256_cap", float, 16, 8, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("directf32_32x16_t8x8_th256_cap", float, 32, 16, 8, 8, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x32_t8x8_th256_cap", float, 64, 32, 8, 8, 256, false),
-    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r1024_u1_gram", double, 4, 4, 4, 4, 8, 6, 1024, 1, true, true),
+    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s3_r2048_u1_gram", double, 4, 4, 4, 4, 8, 3, 2048, 1, true, true),
 };
 extern const int kGenPart6Count;
 const int kGenPart6Count = 38;

@@ -44,7 +44,7 @@ const Variant kGenPart7[] = {
     TSM_DIRECT_VARIANT("directf32_16x16_t8x8_th256_cap", float, 16, 16, 8, 8, 256, false),
     TSM_DIRECT_VARIANT("directf32_32x32_t8x8_th256_cap", float, 32, 32, 8, 8, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x64_t8x8_th256_cap", float, 64, 64, 8, 8, 256, false),
-    TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s6_r512_u1_gram", double, 8, 8, 4, 4, 8, 6, 512, 1, true, true),
+    TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s3_r1024_u1_gram", double, 8, 8, 4, 4, 8, 3, 1024, 1, true, true),
 };
 extern const int kGenPart7Count;
 const int kGenPart7Count = 38;
