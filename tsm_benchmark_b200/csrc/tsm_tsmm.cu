@@ -52,7 +52,9 @@ struct DmmaEntry {
 
 template <typename T, int P>
 constexpr int dmma_rows() {
-  return 32768 / (P * int(sizeof(T)));
+  // FP32 X with P >= 16: 64 KB stages (one CTA per SM by occupancy), 5-7 %
+  // faster than 32 KB at 16 x 16 and 32 x 32, 5 % slower at 8 x 8.
+  return (sizeof(T) == 4 && P >= 16 ? 65536 : 32768) / (P * int(sizeof(T)));
 }
 
 #define TSM_DMMA_ENTRY(T, DT, P, Q)                                                                            \
