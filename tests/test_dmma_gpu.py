@@ -26,11 +26,13 @@ def test_sixteen_dmma_variants_exist(gpu):
 @pytest.mark.parametrize("k", [16, 32, 48, 64])
 def test_dmma_variant_parity(gpu, oracle_mod, m, k):
     from tsm_benchmark_b200 import tsmttsm
-    (v,) = [v for v in dmma_variants() if (v["wa"], v["wb"]) == (m, k)]
-    for n in (0, 1, 5, v["rows"] - 1, v["rows"] + 3, 3 * v["rows"] + 11, 40013):
-        A, B = oracle_mod.operands(n, m, k, 100 + n % 97 + m + k)
-        C = tsmttsm(to_dev(A, gpu), to_dev(B, gpu), variant=v["index"])
-        assert_parity(oracle_mod, A, B, C, what=f"{v['name']} n={n}")
+    vs = [v for v in dmma_variants() if (v["wa"], v["wb"]) == (m, k)]  # every ring shape of the pair
+    assert vs
+    for v in vs:
+        for n in (0, 1, 5, v["rows"] - 1, v["rows"] + 3, 3 * v["rows"] + 11, 40013):
+            A, B = oracle_mod.operands(n, m, k, 100 + n % 97 + m + k)
+            C = tsmttsm(to_dev(A, gpu), to_dev(B, gpu), variant=v["index"])
+            assert_parity(oracle_mod, A, B, C, what=f"{v['name']} n={n}")
 
 
 def test_dmma_strided_operands(gpu, oracle_mod):

@@ -389,6 +389,9 @@ def default_variants() -> list:
         out.append(dataclasses.replace(g, stages=3, rows=2 * g.resolved().rows))
     for w in (1, 2, 4, 8):
         out.append(BulkVariant(w, w, default_tile(w), default_tile(w), gram=True))
+    # FP64 tensor-core kernels with other ring shapes (autotuner candidates)
+    for wa, rows, stages in ((16, 192, 4), (16, 128, 6), (32, 96, 4), (32, 192, 2), (32, 64, 6)):
+        out.append(DmmaVariant(wa, wa, rows=rows, stages=stages))
     return out
 
 

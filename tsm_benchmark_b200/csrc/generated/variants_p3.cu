@@ -46,8 +46,9 @@ const Variant kGenPart3[] = {
     TSM_DIRECT_VARIANT("directf32_32x4_t8x4_th256_cap", float, 32, 4, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x8_t8x4_th256_cap", float, 64, 8, 8, 4, 256, false),
     TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s3_r8192_u1_gram", double, 1, 1, 1, 1, 8, 3, 8192, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s4_r192", 16, 16, 2, 2, 8, 4, 192),
 };
 extern const int kGenPart3Count;
-const int kGenPart3Count = 39;
+const int kGenPart3Count = 40;
 
 }  // namespace tsm

@@ -46,8 +46,9 @@ const Variant kGenPart4[] = {
     TSM_DIRECT_VARIANT("directf32_32x8_t8x4_th256_cap", float, 32, 8, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x16_t8x8_th256_cap", float, 64, 16, 8, 8, 256, false),
     TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s3_r4096_u1_gram", double, 2, 2, 2, 2, 8, 3, 4096, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s6_r128", 16, 16, 2, 2, 8, 6, 128),
 };
 extern const int kGenPart4Count;
-const int kGenPart4Count = 39;
+const int kGenPart4Count = 40;
 
 }  // namespace tsm

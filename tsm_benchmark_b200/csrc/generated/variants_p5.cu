@@ -46,8 +46,9 @@ const Variant kGenPart5[] = {
     TSM_DIRECT_VARIANT("directf32_32x16_t8x8_th256_cap", float, 32, 16, 8, 8, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x32_t8x8_th256_cap", float, 64, 32, 8, 8, 256, false),
     TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s3_r2048_u1_gram", double, 4, 4, 4, 4, 8, 3, 2048, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s4_r96", 32, 32, 4, 4, 8, 4, 96),
 };
 extern const int kGenPart5Count;
-const int kGenPart5Count = 39;
+const int kGenPart5Count = 40;
 
 }  // namespace tsm

@@ -46,8 +46,9 @@ const Variant kGenPart6[] = {
     TSM_DIRECT_VARIANT("directf32_32x32_t8x8_th256_cap", float, 32, 32, 8, 8, 256, false),
     TSM_DIRECT_VARIANT("directf32_64x64_t8x8_th256_cap", float, 64, 64, 8, 8, 256, false),
     TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s3_r1024_u1_gram", double, 8, 8, 4, 4, 8, 3, 1024, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s2_r192", 32, 32, 4, 4, 8, 2, 192),
 };
 extern const int kGenPart6Count;
-const int kGenPart6Count = 39;
+const int kGenPart6Count = 40;
 
 }  // namespace tsm

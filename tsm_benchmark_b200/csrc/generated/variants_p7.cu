@@ -46,8 +46,9 @@ const Variant kGenPart7[] = {
     TSM_DIRECT_VARIANT("directf32_32x64_t8x8_th256_cap", float, 32, 64, 8, 8, 256, false),
     TSM_GRAM_DMMA_VARIANT("dmma_16x16_gram_w8_s4_r256", 16, 8, 4, 256),
     TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r4096_u1_gram", double, 1, 1, 1, 1, 8, 6, 4096, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s6_r64", 32, 32, 4, 4, 8, 6, 64),
 };
 extern const int kGenPart7Count;
-const int kGenPart7Count = 39;
+const int kGenPart7Count = 40;
 
 }  // namespace tsm
