@@ -68,7 +68,7 @@ def test_fused_backward(gpu, oracle_mod, dtype, m, k):
 
 
 def test_gradcheck_fp64(gpu):
-    """BASELINE's check: n = 2^12, m = k = 4, FP64, finite differences."""
+    """The gradient check of the differentiation form: n = 2^12, m = k = 4, FP64, finite differences."""
     from tsm_benchmark_b200 import gram_tn
     g = torch.Generator(device=gpu).manual_seed(0)
     A = torch.rand((1 << 12, 4), dtype=torch.float64, device=gpu, generator=g).requires_grad_()
@@ -78,7 +78,7 @@ def test_gradcheck_fp64(gpu):
 
 @pytest.mark.parametrize("dtype,rtol", [(torch.float64, 1e-12), (torch.float32, 2e-5)])
 def test_matches_torch_gradient(gpu, dtype, rtol):
-    """loss = sum(W * C), W an m x k normal matrix (BASELINE's loss), n = 2^22,
+    """loss = sum(W * C), W an m x k normal matrix (the differentiation form's loss), n = 2^22,
     m = k = 16: forward and both gradients against torch's A.T @ B."""
     from tsm_benchmark_b200 import gram_tn
     g = torch.Generator(device=gpu).manual_seed(1)

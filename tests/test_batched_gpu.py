@@ -87,7 +87,7 @@ def test_batched_rejects_other_widths(gpu):
 
 
 def test_batched_full_config_against_plain(gpu, oracle_mod):
-    """BASELINE's batched configuration: 512 problems, n log-uniform in
+    """The batched form's configuration: 512 problems, n log-uniform in
     [10^3, 10^6], widths in {4, 8, 16, 32}; every C_p equals the plain path's
     within the normwise bound."""
     from tsm_benchmark_b200 import BatchedTSMTTSM, tsmttsm

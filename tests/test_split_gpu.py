@@ -61,7 +61,7 @@ def test_split_deterministic_and_accumulate(gpu):
 
 
 def test_split_full_config(gpu):
-    """BASELINE's precision configuration: n = 2^25, m = k = 32, scaled
+    """The precision form's configuration: n = 2^25, m = k = 32, scaled
     normal FP32 data; error against the plain FP64 path on FP64 copies."""
     from tsm_benchmark_b200 import tsmttsm, tsmttsm_split
     n, w = 1 << 25, 32
