@@ -314,7 +314,7 @@ EXTRA_CANDIDATES: dict[tuple[int, int], list[dict]] = {
     (8, 8): [dict(ta=8, tb=8), dict(unroll=2), dict(ta=2, tb=8),
              # the headline shape: the 2 x 8 tile with other ring shapes
              dict(ta=2, tb=8, stages=3, rows=512), dict(ta=2, tb=8, stages=4, rows=384),
-             dict(ta=2, tb=8, stages=10, rows=128)],
+             dict(ta=2, tb=8, stages=10, rows=128), dict(ta=2, tb=8, stages=2, rows=768)],
     (16, 16): [dict(ta=4, tb=4), dict(ta=4, tb=8)],
     (32, 32): [dict(ta=8, tb=4), dict(cw=16)],
     (64, 64): [dict(unroll=2), dict(stages=4)],
@@ -344,11 +344,11 @@ def default_variants() -> list:
         out.append(base)
         for extra in EXTRA_CANDIDATES.get((wa, wb), []):
             out.append(dataclasses.replace(base, **extra))
-        # Larger ring stages: 3 x ~64 KB and 4 x ~48 KB instead of 6 x ~32 KB
+        # Larger ring stages: 3 x ~64 KB, 4 x ~48 KB, 2 x ~96 KB instead of 6 x ~32 KB
         # (longer contiguous bulk copies; the 8 x 8 headline streamed 6.5 %
         # faster with 3 x 64 KB).
         rows = base.resolved().rows
-        for stages, mult in ((3, 2.0), (4, 1.5)):
+        for stages, mult in ((3, 2.0), (4, 1.5), (2, 3.0)):
             v = dataclasses.replace(base, stages=stages, rows=int(rows * mult))
             v = dataclasses.replace(v, rows=_round_rows(v))
             if not v.validate() and v.name not in {u.name for u in out}:

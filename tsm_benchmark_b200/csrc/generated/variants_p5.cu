@@ -9,46 +9,48 @@ extern const Variant kGenPart5[];
 const Variant kGenPart5[] = {
     TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s3_r128", 32, 32, 4, 4, 8, 3, 128),
     TSM_DMMA_VARIANT("dmma_64x32_t32x32_w8_s3_r80", 64, 32, 4, 4, 8, 3, 80),
-    TSM_BULK_VARIANT("bulk_1x64_t1x8_w8_s6_r32_u1", double, 1, 64, 1, 8, 8, 6, 32, 1, true, false),
-    TSM_BULK_VARIANT("bulk_4x4_t2x2_w8_s6_r512_u1", double, 4, 4, 2, 2, 8, 6, 512, 1, true, false),
-    TSM_BULK_VARIANT("bulk_4x16_t4x8_w8_s3_r256_u1", double, 4, 16, 4, 8, 8, 3, 256, 1, true, false),
+    TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s2_r6144_u1", double, 1, 1, 1, 1, 8, 2, 6144, 1, true, false),
+    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s4_r1536_u1", double, 2, 2, 2, 2, 8, 4, 1536, 1, true, false),
+    TSM_BULK_VARIANT("bulk_4x8_t4x4_w8_s6_r256_u1", double, 4, 8, 4, 4, 8, 6, 256, 1, true, false),
+    TSM_BULK_VARIANT("bulk_4x32_t4x8_w8_s6_r64_u1", double, 4, 32, 4, 8, 8, 6, 64, 1, true, false),
     TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s6_r256_u1", double, 8, 8, 4, 4, 8, 6, 256, 1, true, false),
-    TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s4_r384_u1", double, 8, 8, 4, 4, 8, 4, 384, 1, true, false),
-    TSM_BULK_VARIANT("bulk_16x4_t8x4_w8_s3_r256_u1", double, 16, 4, 8, 4, 8, 3, 256, 1, true, false),
-    TSM_BULK_VARIANT("bulk_16x16_t8x8_w8_s3_r256_u1", double, 16, 16, 8, 8, 8, 3, 256, 1, true, false),
-    TSM_BULK_VARIANT("bulk_32x8_t8x4_w8_s6_r96_u1", double, 32, 8, 8, 4, 8, 6, 96, 1, true, false),
-    TSM_BULK_VARIANT("bulk_32x32_t8x8_w16_s6_r64_u1", double, 32, 32, 8, 8, 16, 6, 64, 1, true, false),
-    TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r2048_u1_cap", double, 1, 1, 1, 1, 8, 6, 2048, 1, false, false),
-    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r1024_u1_cap", double, 2, 2, 2, 2, 8, 6, 1024, 1, false, false),
-    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r512_u1_cap", double, 4, 4, 4, 4, 8, 6, 512, 1, false, false),
-    TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s6_r256_u1_cap", double, 8, 8, 4, 4, 8, 6, 256, 1, false, false),
-    TSM_BULK_VARIANT("bulk_16x16_t8x8_w8_s6_r128_u1_cap", double, 16, 16, 8, 8, 8, 6, 128, 1, false, false),
-    TSM_BULK_VARIANT("bulk_32x32_t8x8_w8_s6_r64_u1_cap", double, 32, 32, 8, 8, 8, 6, 64, 1, false, false),
-    TSM_BULK_VARIANT("bulk_64x64_t8x8_w8_s6_r32_u1_cap", double, 64, 64, 8, 8, 8, 6, 32, 1, false, false),
-    TSM_DIRECT_VARIANT("direct_2x1_t2x1_th256_cap", double, 2, 1, 2, 1, 256, false),
-    TSM_DIRECT_VARIANT("direct_4x2_t4x2_th256_cap", double, 4, 2, 4, 2, 256, false),
-    TSM_DIRECT_VARIANT("direct_8x4_t4x4_th256_cap", double, 8, 4, 4, 4, 256, false),
-    TSM_DIRECT_VARIANT("direct_16x8_t8x4_th256_cap", double, 16, 8, 8, 4, 256, false),
-    TSM_DIRECT_VARIANT("direct_32x16_t8x8_th256_cap", double, 32, 16, 8, 8, 256, false),
-    TSM_DIRECT_VARIANT("direct_64x32_t8x8_th256_cap", double, 64, 32, 8, 8, 256, false),
-    TSM_BULK_VARIANT("bulkf32_64x64_t8x8_w8_s3_r128_u1", float, 64, 64, 8, 8, 8, 3, 128, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_1x1_t1x1_w8_s6_r4096_u1_cap", float, 1, 1, 1, 1, 8, 6, 4096, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_2x2_t2x2_w8_s6_r2048_u1_cap", float, 2, 2, 2, 2, 8, 6, 2048, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_4x4_t4x4_w8_s6_r1024_u1_cap", float, 4, 4, 4, 4, 8, 6, 1024, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_8x8_t4x4_w8_s6_r512_u1_cap", float, 8, 8, 4, 4, 8, 6, 512, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_16x16_t8x8_w8_s6_r256_u1_cap", float, 16, 16, 8, 8, 8, 6, 256, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_32x32_t8x8_w8_s6_r128_u1_cap", float, 32, 32, 8, 8, 8, 6, 128, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_64x64_t8x8_w8_s6_r64_u1_cap", float, 64, 64, 8, 8, 8, 6, 64, 1, false, false),
-    TSM_DIRECT_VARIANT("directf32_2x1_t2x1_th256_cap", float, 2, 1, 2, 1, 256, false),
-    TSM_DIRECT_VARIANT("directf32_4x2_t4x2_th256_cap", float, 4, 2, 4, 2, 256, false),
-    TSM_DIRECT_VARIANT("directf32_8x4_t4x4_th256_cap", float, 8, 4, 4, 4, 256, false),
-    TSM_DIRECT_VARIANT("directf32_16x8_t8x4_th256_cap", float, 16, 8, 8, 4, 256, false),
-    TSM_DIRECT_VARIANT("directf32_32x16_t8x8_th256_cap", float, 32, 16, 8, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_64x32_t8x8_th256_cap", float, 64, 32, 8, 8, 256, false),
-    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s3_r2048_u1_gram", double, 4, 4, 4, 4, 8, 3, 2048, 1, true, true),
-    TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s4_r96", 32, 32, 4, 4, 8, 4, 96),
+    TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s3_r512_u1", double, 8, 8, 4, 4, 8, 3, 512, 1, true, false),
+    TSM_BULK_VARIANT("bulk_8x32_t4x8_w8_s3_r192_u1", double, 8, 32, 4, 8, 8, 3, 192, 1, true, false),
+    TSM_BULK_VARIANT("bulk_16x8_t8x4_w8_s3_r256_u1", double, 16, 8, 8, 4, 8, 3, 256, 1, true, false),
+    TSM_BULK_VARIANT("bulk_16x16_t8x8_w8_s2_r384_u1", double, 16, 16, 8, 8, 8, 2, 384, 1, true, false),
+    TSM_BULK_VARIANT("bulk_32x4_t8x4_w8_s2_r192_u1", double, 32, 4, 8, 4, 8, 2, 192, 1, true, false),
+    TSM_BULK_VARIANT("bulk_32x16_t8x8_w8_s2_r192_u1", double, 32, 16, 8, 8, 8, 2, 192, 1, true, false),
+    TSM_BULK_VARIANT("bulk_64x64_t8x8_w8_s6_r32_u2", double, 64, 64, 8, 8, 8, 6, 32, 2, true, false),
+    TSM_BULK_VARIANT("bulk_1x8_t1x4_w8_s6_r384_u1_cap", double, 1, 8, 1, 4, 8, 6, 384, 1, false, false),
+    TSM_BULK_VARIANT("bulk_2x16_t2x8_w8_s6_r128_u1_cap", double, 2, 16, 2, 8, 8, 6, 128, 1, false, false),
+    TSM_BULK_VARIANT("bulk_4x32_t4x8_w8_s6_r64_u1_cap", double, 4, 32, 4, 8, 8, 6, 64, 1, false, false),
+    TSM_BULK_VARIANT("bulk_8x64_t4x8_w8_s6_r48_u1_cap", double, 8, 64, 4, 8, 8, 6, 48, 1, false, false),
+    TSM_BULK_VARIANT("bulk_32x1_t8x1_w8_s6_r64_u1_cap", double, 32, 1, 8, 1, 8, 6, 64, 1, false, false),
+    TSM_BULK_VARIANT("bulk_64x2_t8x2_w8_s6_r32_u1_cap", double, 64, 2, 8, 2, 8, 6, 32, 1, false, false),
+    TSM_DIRECT_VARIANT("direct_1x4_t1x4_th256_cap", double, 1, 4, 1, 4, 256, false),
+    TSM_DIRECT_VARIANT("direct_2x8_t2x4_th256_cap", double, 2, 8, 2, 4, 256, false),
+    TSM_DIRECT_VARIANT("direct_4x16_t4x8_th256_cap", double, 4, 16, 4, 8, 256, false),
+    TSM_DIRECT_VARIANT("direct_8x32_t4x8_th256_cap", double, 8, 32, 4, 8, 256, false),
+    TSM_DIRECT_VARIANT("direct_16x64_t8x8_th256_cap", double, 16, 64, 8, 8, 256, false),
+    TSM_DIRECT_VARIANT("direct_64x1_t8x1_th256_cap", double, 64, 1, 8, 1, 256, false),
+    TSM_BULK_VARIANT("bulkf32_2x2_t2x2_w8_s3_r4096_u1", float, 2, 2, 2, 2, 8, 3, 4096, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_4x4_t4x4_w8_s6_r1024_u1", float, 4, 4, 4, 4, 8, 6, 1024, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_1x8_t1x4_w8_s6_r896_u1_cap", float, 1, 8, 1, 4, 8, 6, 896, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_2x16_t2x8_w8_s6_r384_u1_cap", float, 2, 16, 2, 8, 8, 6, 384, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_4x32_t4x8_w8_s6_r192_u1_cap", float, 4, 32, 4, 8, 8, 6, 192, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_8x64_t4x8_w8_s6_r112_u1_cap", float, 8, 64, 4, 8, 8, 6, 112, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_32x1_t8x1_w8_s6_r192_u1_cap", float, 32, 1, 8, 1, 8, 6, 192, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_64x2_t8x2_w8_s6_r96_u1_cap", float, 64, 2, 8, 2, 8, 6, 96, 1, false, false),
+    TSM_DIRECT_VARIANT("directf32_1x4_t1x4_th256_cap", float, 1, 4, 1, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_2x8_t2x4_th256_cap", float, 2, 8, 2, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_4x16_t4x8_th256_cap", float, 4, 16, 4, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_8x32_t4x8_th256_cap", float, 8, 32, 4, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_16x64_t8x8_th256_cap", float, 16, 64, 8, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_64x1_t8x1_th256_cap", float, 64, 1, 8, 1, 256, false),
+    TSM_GRAM_DMMA_VARIANT("dmma_32x32_gram_w8_s3_r256", 32, 8, 3, 256),
+    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r2048_u1_gram", double, 2, 2, 2, 2, 8, 6, 2048, 1, true, true),
 };
 extern const int kGenPart5Count;
-const int kGenPart5Count = 40;
+const int kGenPart5Count = 42;
 
 }  // namespace tsm
