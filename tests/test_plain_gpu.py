@@ -226,3 +226,26 @@ def test_parity_fp32_storage(gpu, oracle_mod, m, k):
         assert err <= bound + 1e-30, (n, m, k, err, bound)
     names = [v for v in variants() if v["dtype"] == "f32"]
     assert names
+
+
+def test_every_fp32_exact_variant(gpu, oracle_mod):
+    """Every FP32-storage exact square, each ring shape (2, 3 and 6 stages),
+    on a ragged row count and on one shorter than a chunk, with the bound of
+    the FP32 parity test."""
+    from tsm_benchmark_b200 import tsmttsm, variants
+    ran = 0
+    for v in variants():
+        if v["dtype"] != "f32" or not v["exact"] or v["kind"] != "bulk":
+            continue
+        m = k = v["wa"]
+        for n in (v["rows"] - 3, 100003):
+            A, B = oracle_mod.operands(n, m, k, seed=91 + m + n)
+            A32, B32 = A.astype(np.float32), B.astype(np.float32)
+            C = tsmttsm(to_dev(A32, gpu), to_dev(B32, gpu), variant=v["index"])
+            ref = oracle_mod.naive(A32, B32)
+            err = np.linalg.norm(C.cpu().numpy().astype(np.float64) - ref)
+            per_thread = max(1, n // (148 * 8)) + 2
+            bound = 2.0**-24 * per_thread * np.linalg.norm(A32.astype(np.float64)) * np.linalg.norm(B32.astype(np.float64))
+            assert err <= bound + 1e-30, (v["name"], n, err, bound)
+        ran += 1
+    assert ran >= 21

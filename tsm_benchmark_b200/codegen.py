@@ -361,14 +361,18 @@ def default_variants() -> list:
             out.append(DirectVariant(wa, wb, default_tile(wa), default_tile(wb)))
     # FP32 storage (FP32 per-thread accumulation, FP64 reductions): exact
     # squares, then capacities, then direct loads, in the same order.
-    # FP32 exact squares: 3 stages of twice the rows first (the FP32 default
-    # is the first applicable variant; against 6 stages they streamed 2-9 %
-    # faster at n = 2^22-2^25), then the 6-stage ones.
-    for w in WIDTH_CAPS:
-        g = BulkVariant(w, w, default_tile(w), default_tile(w), dtype="f32")
-        v = dataclasses.replace(g, stages=3, rows=2 * g.resolved().rows)
-        if not v.validate():
-            out.append(v)
+    # FP32 exact squares: 2 stages of three times the rows first, then 3
+    # stages of twice the rows, then the 6-stage ones (the FP32 default is
+    # the first applicable variant; in interleaved timings at n = 2^22-2^25,
+    # 3 stages streamed 2-9 % faster than 6 and 2 stages up to 7 % faster
+    # than 3).
+    for stages, mult in ((2, 3), (3, 2)):
+        for w in WIDTH_CAPS:
+            g = BulkVariant(w, w, default_tile(w), default_tile(w), dtype="f32")
+            v = dataclasses.replace(g, stages=stages, rows=mult * g.resolved().rows)
+            v = dataclasses.replace(v, rows=_round_rows(v))
+            if not v.validate():
+                out.append(v)
     for w in WIDTH_CAPS:
         out.append(BulkVariant(w, w, default_tile(w), default_tile(w), dtype="f32"))
     for wa in WIDTH_CAPS:
@@ -381,12 +385,17 @@ def default_variants() -> list:
     # tensor cores for the DMMA widths, SIMT register tiles below 16.
     for w in DMMA_WIDTHS:
         out.append(DmmaVariant(w, w, gram=True))
-    # SIMT Gram kernels, 3 stages of ~64 KB first (the default takes the first
-    # applicable Gram variant; against 6 stages of ~32 KB they streamed A 3-11 %
-    # faster at n = 2^26), the 6-stage ones after them.
-    for w in (1, 2, 4, 8):
-        g = BulkVariant(w, w, default_tile(w), default_tile(w), gram=True)
-        out.append(dataclasses.replace(g, stages=3, rows=2 * g.resolved().rows))
+    # SIMT Gram kernels, 2 stages of ~96 KB first, then 3 of ~64 KB, the
+    # 6-stage ones last (the default takes the first applicable Gram variant;
+    # in interleaved timings at n = 2^26, 3 stages streamed A 3-11 % faster
+    # than 6 and 2 stages 1.5-8 % faster than 3).
+    for stages, mult in ((2, 3), (3, 2)):
+        for w in (1, 2, 4, 8):
+            g = BulkVariant(w, w, default_tile(w), default_tile(w), gram=True)
+            v = dataclasses.replace(g, stages=stages, rows=mult * g.resolved().rows)
+            v = dataclasses.replace(v, rows=_round_rows(v))
+            if not v.validate():
+                out.append(v)
     for w in (1, 2, 4, 8):
         out.append(BulkVariant(w, w, default_tile(w), default_tile(w), gram=True))
     # FP64 tensor-core kernels with other ring shapes (autotuner candidates)

@@ -34,24 +34,25 @@ const Variant kGenPart0[] = {
     TSM_DIRECT_VARIANT("direct_16x2_t8x2_th256_cap", double, 16, 2, 8, 2, 256, false),
     TSM_DIRECT_VARIANT("direct_32x4_t8x4_th256_cap", double, 32, 4, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("direct_64x8_t8x4_th256_cap", double, 64, 8, 8, 4, 256, false),
-    TSM_BULK_VARIANT("bulkf32_16x16_t8x8_w8_s3_r512_u1", float, 16, 16, 8, 8, 8, 3, 512, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_32x32_t8x8_w8_s6_r128_u1", float, 32, 32, 8, 8, 8, 6, 128, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_1x64_t1x8_w8_s6_r96_u1_cap", float, 1, 64, 1, 8, 8, 6, 96, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_4x1_t4x1_w8_s6_r1536_u1_cap", float, 4, 1, 4, 1, 8, 6, 1536, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_8x2_t4x2_w8_s6_r768_u1_cap", float, 8, 2, 4, 2, 8, 6, 768, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_16x4_t8x4_w8_s6_r384_u1_cap", float, 16, 4, 8, 4, 8, 6, 384, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_32x8_t8x4_w8_s6_r192_u1_cap", float, 32, 8, 8, 4, 8, 6, 192, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_64x16_t8x8_w8_s6_r96_u1_cap", float, 64, 16, 8, 8, 8, 6, 96, 1, false, false),
-    TSM_DIRECT_VARIANT("directf32_1x32_t1x8_th256_cap", float, 1, 32, 1, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_2x64_t2x8_th256_cap", float, 2, 64, 2, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_8x1_t4x1_th256_cap", float, 8, 1, 4, 1, 256, false),
-    TSM_DIRECT_VARIANT("directf32_16x2_t8x2_th256_cap", float, 16, 2, 8, 2, 256, false),
-    TSM_DIRECT_VARIANT("directf32_32x4_t8x4_th256_cap", float, 32, 4, 8, 4, 256, false),
-    TSM_DIRECT_VARIANT("directf32_64x8_t8x4_th256_cap", float, 64, 8, 8, 4, 256, false),
-    TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s3_r8192_u1_gram", double, 1, 1, 1, 1, 8, 3, 8192, 1, true, true),
-    TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s4_r192", 16, 16, 2, 2, 8, 4, 192),
+    TSM_BULK_VARIANT("bulkf32_16x16_t8x8_w8_s2_r768_u1", float, 16, 16, 8, 8, 8, 2, 768, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_32x32_t8x8_w8_s3_r256_u1", float, 32, 32, 8, 8, 8, 3, 256, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_64x64_t8x8_w8_s6_r64_u1", float, 64, 64, 8, 8, 8, 6, 64, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_2x1_t2x1_w8_s6_r2560_u1_cap", float, 2, 1, 2, 1, 8, 6, 2560, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_4x2_t4x2_w8_s6_r1280_u1_cap", float, 4, 2, 4, 2, 8, 6, 1280, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_8x4_t4x4_w8_s6_r640_u1_cap", float, 8, 4, 4, 4, 8, 6, 640, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_16x8_t8x4_w8_s6_r320_u1_cap", float, 16, 8, 8, 4, 8, 6, 320, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_32x16_t8x8_w8_s6_r160_u1_cap", float, 32, 16, 8, 8, 8, 6, 160, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_64x32_t8x8_w8_s6_r80_u1_cap", float, 64, 32, 8, 8, 8, 6, 80, 1, false, false),
+    TSM_DIRECT_VARIANT("directf32_1x64_t1x8_th256_cap", float, 1, 64, 1, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_4x1_t4x1_th256_cap", float, 4, 1, 4, 1, 256, false),
+    TSM_DIRECT_VARIANT("directf32_8x2_t4x2_th256_cap", float, 8, 2, 4, 2, 256, false),
+    TSM_DIRECT_VARIANT("directf32_16x4_t8x4_th256_cap", float, 16, 4, 8, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_32x8_t8x4_th256_cap", float, 32, 8, 8, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_64x16_t8x8_th256_cap", float, 64, 16, 8, 8, 256, false),
+    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s2_r6144_u1_gram", double, 2, 2, 2, 2, 8, 2, 6144, 1, true, true),
+    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r2048_u1_gram", double, 2, 2, 2, 2, 8, 6, 2048, 1, true, true),
 };
 extern const int kGenPart0Count;
-const int kGenPart0Count = 43;
+const int kGenPart0Count = 44;
 
 }  // namespace tsm

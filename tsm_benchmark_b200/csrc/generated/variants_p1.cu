@@ -34,24 +34,25 @@ const Variant kGenPart1[] = {
     TSM_DIRECT_VARIANT("direct_16x4_t8x4_th256_cap", double, 16, 4, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("direct_32x8_t8x4_th256_cap", double, 32, 8, 8, 4, 256, false),
     TSM_DIRECT_VARIANT("direct_64x16_t8x8_th256_cap", double, 64, 16, 8, 8, 256, false),
-    TSM_BULK_VARIANT("bulkf32_32x32_t8x8_w8_s3_r256_u1", float, 32, 32, 8, 8, 8, 3, 256, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_64x64_t8x8_w8_s6_r64_u1", float, 64, 64, 8, 8, 8, 6, 64, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_2x1_t2x1_w8_s6_r2560_u1_cap", float, 2, 1, 2, 1, 8, 6, 2560, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_4x2_t4x2_w8_s6_r1280_u1_cap", float, 4, 2, 4, 2, 8, 6, 1280, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_8x4_t4x4_w8_s6_r640_u1_cap", float, 8, 4, 4, 4, 8, 6, 640, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_16x8_t8x4_w8_s6_r320_u1_cap", float, 16, 8, 8, 4, 8, 6, 320, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_32x16_t8x8_w8_s6_r160_u1_cap", float, 32, 16, 8, 8, 8, 6, 160, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_64x32_t8x8_w8_s6_r80_u1_cap", float, 64, 32, 8, 8, 8, 6, 80, 1, false, false),
-    TSM_DIRECT_VARIANT("directf32_1x64_t1x8_th256_cap", float, 1, 64, 1, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_4x1_t4x1_th256_cap", float, 4, 1, 4, 1, 256, false),
-    TSM_DIRECT_VARIANT("directf32_8x2_t4x2_th256_cap", float, 8, 2, 4, 2, 256, false),
-    TSM_DIRECT_VARIANT("directf32_16x4_t8x4_th256_cap", float, 16, 4, 8, 4, 256, false),
-    TSM_DIRECT_VARIANT("directf32_32x8_t8x4_th256_cap", float, 32, 8, 8, 4, 256, false),
-    TSM_DIRECT_VARIANT("directf32_64x16_t8x8_th256_cap", float, 64, 16, 8, 8, 256, false),
-    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s3_r4096_u1_gram", double, 2, 2, 2, 2, 8, 3, 4096, 1, true, true),
-    TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s6_r128", 16, 16, 2, 2, 8, 6, 128),
+    TSM_BULK_VARIANT("bulkf32_32x32_t8x8_w8_s2_r384_u1", float, 32, 32, 8, 8, 8, 2, 384, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_64x64_t8x8_w8_s3_r128_u1", float, 64, 64, 8, 8, 8, 3, 128, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_1x1_t1x1_w8_s6_r4096_u1_cap", float, 1, 1, 1, 1, 8, 6, 4096, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_2x2_t2x2_w8_s6_r2048_u1_cap", float, 2, 2, 2, 2, 8, 6, 2048, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_4x4_t4x4_w8_s6_r1024_u1_cap", float, 4, 4, 4, 4, 8, 6, 1024, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_8x8_t4x4_w8_s6_r512_u1_cap", float, 8, 8, 4, 4, 8, 6, 512, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_16x16_t8x8_w8_s6_r256_u1_cap", float, 16, 16, 8, 8, 8, 6, 256, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_32x32_t8x8_w8_s6_r128_u1_cap", float, 32, 32, 8, 8, 8, 6, 128, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_64x64_t8x8_w8_s6_r64_u1_cap", float, 64, 64, 8, 8, 8, 6, 64, 1, false, false),
+    TSM_DIRECT_VARIANT("directf32_2x1_t2x1_th256_cap", float, 2, 1, 2, 1, 256, false),
+    TSM_DIRECT_VARIANT("directf32_4x2_t4x2_th256_cap", float, 4, 2, 4, 2, 256, false),
+    TSM_DIRECT_VARIANT("directf32_8x4_t4x4_th256_cap", float, 8, 4, 4, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_16x8_t8x4_th256_cap", float, 16, 8, 8, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_32x16_t8x8_th256_cap", float, 32, 16, 8, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_64x32_t8x8_th256_cap", float, 64, 32, 8, 8, 256, false),
+    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s2_r3072_u1_gram", double, 4, 4, 4, 4, 8, 2, 3072, 1, true, true),
+    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r1024_u1_gram", double, 4, 4, 4, 4, 8, 6, 1024, 1, true, true),
 };
 extern const int kGenPart1Count;
-const int kGenPart1Count = 43;
+const int kGenPart1Count = 44;
 
 }  // namespace tsm

@@ -33,24 +33,26 @@ const Variant kGenPart5[] = {
     TSM_DIRECT_VARIANT("direct_8x32_t4x8_th256_cap", double, 8, 32, 4, 8, 256, false),
     TSM_DIRECT_VARIANT("direct_16x64_t8x8_th256_cap", double, 16, 64, 8, 8, 256, false),
     TSM_DIRECT_VARIANT("direct_64x1_t8x1_th256_cap", double, 64, 1, 8, 1, 256, false),
-    TSM_BULK_VARIANT("bulkf32_2x2_t2x2_w8_s3_r4096_u1", float, 2, 2, 2, 2, 8, 3, 4096, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_4x4_t4x4_w8_s6_r1024_u1", float, 4, 4, 4, 4, 8, 6, 1024, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_1x8_t1x4_w8_s6_r896_u1_cap", float, 1, 8, 1, 4, 8, 6, 896, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_2x16_t2x8_w8_s6_r384_u1_cap", float, 2, 16, 2, 8, 8, 6, 384, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_4x32_t4x8_w8_s6_r192_u1_cap", float, 4, 32, 4, 8, 8, 6, 192, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_8x64_t4x8_w8_s6_r112_u1_cap", float, 8, 64, 4, 8, 8, 6, 112, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_32x1_t8x1_w8_s6_r192_u1_cap", float, 32, 1, 8, 1, 8, 6, 192, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_64x2_t8x2_w8_s6_r96_u1_cap", float, 64, 2, 8, 2, 8, 6, 96, 1, false, false),
-    TSM_DIRECT_VARIANT("directf32_1x4_t1x4_th256_cap", float, 1, 4, 1, 4, 256, false),
-    TSM_DIRECT_VARIANT("directf32_2x8_t2x4_th256_cap", float, 2, 8, 2, 4, 256, false),
-    TSM_DIRECT_VARIANT("directf32_4x16_t4x8_th256_cap", float, 4, 16, 4, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_8x32_t4x8_th256_cap", float, 8, 32, 4, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_16x64_t8x8_th256_cap", float, 16, 64, 8, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_64x1_t8x1_th256_cap", float, 64, 1, 8, 1, 256, false),
-    TSM_GRAM_DMMA_VARIANT("dmma_32x32_gram_w8_s3_r256", 32, 8, 3, 256),
-    TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r2048_u1_gram", double, 2, 2, 2, 2, 8, 6, 2048, 1, true, true),
+    TSM_BULK_VARIANT("bulkf32_2x2_t2x2_w8_s2_r6144_u1", float, 2, 2, 2, 2, 8, 2, 6144, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_4x4_t4x4_w8_s3_r2048_u1", float, 4, 4, 4, 4, 8, 3, 2048, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_8x8_t4x4_w8_s6_r512_u1", float, 8, 8, 4, 4, 8, 6, 512, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_1x16_t1x8_w8_s6_r384_u1_cap", float, 1, 16, 1, 8, 8, 6, 384, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_2x32_t2x8_w8_s6_r192_u1_cap", float, 2, 32, 2, 8, 8, 6, 192, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_4x64_t4x8_w8_s6_r96_u1_cap", float, 4, 64, 4, 8, 8, 6, 96, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_16x1_t8x1_w8_s6_r384_u1_cap", float, 16, 1, 8, 1, 8, 6, 384, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_32x2_t8x2_w8_s6_r192_u1_cap", float, 32, 2, 8, 2, 8, 6, 192, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_64x4_t8x4_w8_s6_r96_u1_cap", float, 64, 4, 8, 4, 8, 6, 96, 1, false, false),
+    TSM_DIRECT_VARIANT("directf32_1x8_t1x4_th256_cap", float, 1, 8, 1, 4, 256, false),
+    TSM_DIRECT_VARIANT("directf32_2x16_t2x8_th256_cap", float, 2, 16, 2, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_4x32_t4x8_th256_cap", float, 4, 32, 4, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_8x64_t4x8_th256_cap", float, 8, 64, 4, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_32x1_t8x1_th256_cap", float, 32, 1, 8, 1, 256, false),
+    TSM_DIRECT_VARIANT("directf32_64x2_t8x2_th256_cap", float, 64, 2, 8, 2, 256, false),
+    TSM_GRAM_DMMA_VARIANT("dmma_48x48_gram_w8_s3_r160", 48, 8, 3, 160),
+    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s3_r2048_u1_gram", double, 4, 4, 4, 4, 8, 3, 2048, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s4_r96", 32, 32, 4, 4, 8, 4, 96),
 };
 extern const int kGenPart5Count;
-const int kGenPart5Count = 42;
+const int kGenPart5Count = 44;
 
 }  // namespace tsm

@@ -33,24 +33,26 @@ const Variant kGenPart6[] = {
     TSM_DIRECT_VARIANT("direct_8x64_t4x8_th256_cap", double, 8, 64, 4, 8, 256, false),
     TSM_DIRECT_VARIANT("direct_32x1_t8x1_th256_cap", double, 32, 1, 8, 1, 256, false),
     TSM_DIRECT_VARIANT("direct_64x2_t8x2_th256_cap", double, 64, 2, 8, 2, 256, false),
-    TSM_BULK_VARIANT("bulkf32_4x4_t4x4_w8_s3_r2048_u1", float, 4, 4, 4, 4, 8, 3, 2048, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_8x8_t4x4_w8_s6_r512_u1", float, 8, 8, 4, 4, 8, 6, 512, 1, true, false),
-    TSM_BULK_VARIANT("bulkf32_1x16_t1x8_w8_s6_r384_u1_cap", float, 1, 16, 1, 8, 8, 6, 384, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_2x32_t2x8_w8_s6_r192_u1_cap", float, 2, 32, 2, 8, 8, 6, 192, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_4x64_t4x8_w8_s6_r96_u1_cap", float, 4, 64, 4, 8, 8, 6, 96, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_16x1_t8x1_w8_s6_r384_u1_cap", float, 16, 1, 8, 1, 8, 6, 384, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_32x2_t8x2_w8_s6_r192_u1_cap", float, 32, 2, 8, 2, 8, 6, 192, 1, false, false),
-    TSM_BULK_VARIANT("bulkf32_64x4_t8x4_w8_s6_r96_u1_cap", float, 64, 4, 8, 4, 8, 6, 96, 1, false, false),
-    TSM_DIRECT_VARIANT("directf32_1x8_t1x4_th256_cap", float, 1, 8, 1, 4, 256, false),
-    TSM_DIRECT_VARIANT("directf32_2x16_t2x8_th256_cap", float, 2, 16, 2, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_4x32_t4x8_th256_cap", float, 4, 32, 4, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_8x64_t4x8_th256_cap", float, 8, 64, 4, 8, 256, false),
-    TSM_DIRECT_VARIANT("directf32_32x1_t8x1_th256_cap", float, 32, 1, 8, 1, 256, false),
-    TSM_DIRECT_VARIANT("directf32_64x2_t8x2_th256_cap", float, 64, 2, 8, 2, 256, false),
-    TSM_GRAM_DMMA_VARIANT("dmma_48x48_gram_w8_s3_r160", 48, 8, 3, 160),
-    TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r1024_u1_gram", double, 4, 4, 4, 4, 8, 6, 1024, 1, true, true),
+    TSM_BULK_VARIANT("bulkf32_4x4_t4x4_w8_s2_r3072_u1", float, 4, 4, 4, 4, 8, 2, 3072, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_8x8_t4x4_w8_s3_r1024_u1", float, 8, 8, 4, 4, 8, 3, 1024, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_16x16_t8x8_w8_s6_r256_u1", float, 16, 16, 8, 8, 8, 6, 256, 1, true, false),
+    TSM_BULK_VARIANT("bulkf32_1x32_t1x8_w8_s6_r192_u1_cap", float, 1, 32, 1, 8, 8, 6, 192, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_2x64_t2x8_w8_s6_r96_u1_cap", float, 2, 64, 2, 8, 8, 6, 96, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_8x1_t4x1_w8_s6_r896_u1_cap", float, 8, 1, 4, 1, 8, 6, 896, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_16x2_t8x2_w8_s6_r384_u1_cap", float, 16, 2, 8, 2, 8, 6, 384, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_32x4_t8x4_w8_s6_r192_u1_cap", float, 32, 4, 8, 4, 8, 6, 192, 1, false, false),
+    TSM_BULK_VARIANT("bulkf32_64x8_t8x4_w8_s6_r112_u1_cap", float, 64, 8, 8, 4, 8, 6, 112, 1, false, false),
+    TSM_DIRECT_VARIANT("directf32_1x16_t1x8_th256_cap", float, 1, 16, 1, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_2x32_t2x8_th256_cap", float, 2, 32, 2, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_4x64_t4x8_th256_cap", float, 4, 64, 4, 8, 256, false),
+    TSM_DIRECT_VARIANT("directf32_16x1_t8x1_th256_cap", float, 16, 1, 8, 1, 256, false),
+    TSM_DIRECT_VARIANT("directf32_32x2_t8x2_th256_cap", float, 32, 2, 8, 2, 256, false),
+    TSM_DIRECT_VARIANT("directf32_64x4_t8x4_th256_cap", float, 64, 4, 8, 4, 256, false),
+    TSM_GRAM_DMMA_VARIANT("dmma_64x64_gram_w8_s3_r128", 64, 8, 3, 128),
+    TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s3_r1024_u1_gram", double, 8, 8, 4, 4, 8, 3, 1024, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s2_r192", 32, 32, 4, 4, 8, 2, 192),
 };
 extern const int kGenPart6Count;
-const int kGenPart6Count = 42;
+const int kGenPart6Count = 44;
 
 }  // namespace tsm
