@@ -43,17 +43,16 @@ tsm_status strided_fail(cudaError_t e, const char* what) {
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 // Compile-time launch shapes.
-constexpr int pow2_floor(int x) {
-  int p = 1;
-  while (2 * p <= x) p *= 2;
-  return p;
-}
-// SIMT: chunks of ~64 KB (at least 64 values of r), three stages (against six
-// of ~32 KB: 1-3.4 % faster at n = 2^26, 1 x 1 unchanged).
+// SIMT: chunks of up to ~96 KB (whole boxes of 256 values of r above 256,
+// whole warps of r below, at least 64), two stages.  At n = 2^26 three
+// stages of ~64 KB ran 1-3.4 % faster than six of ~32 KB, and two of ~96 KB
+// 2-3.5 % faster again at 2 x 2, 8 x 8, 2 x 32 and 1 x 64 (1 x 1, 4 x 4 and
+// 4 x 16 within 0.5 %).
 constexpr int cm_simt_rs(int wa, int wb) {
-  return std::min(4096, std::max(64, pow2_floor(8192 / (wa + wb))));
+  return 12288 / (wa + wb) >= 256 ? std::min(6144, 12288 / (wa + wb) / 256 * 256)
+                                  : std::max(64, 12288 / (wa + wb) / 32 * 32);
 }
-constexpr int kCmSimtStages = 3;
+constexpr int kCmSimtStages = 2;
 // DMMA: regions of at most 4 x 4 tiles, 8 consumer warps, ~64 KB chunks of
 // whole 16-value groups (boxes of RS + 2 <= 256 values), as many stages as
 // fit 220 KB (2 to 4).
@@ -216,7 +215,9 @@ extern "C" tsm_status tsm_gemm_tn_strided_f64(tsm_stream_t stream, int64_t n, in
   // 2. Column-major operands that tensor maps can describe.
   const bool cm_a = (a_row == 1 || n == 1) && (m == 1 || (a_col >= n && a_col % 2 == 0));
   const bool cm_b = (b_row == 1 || n == 1) && (k == 1 || (b_col >= n && b_col % 2 == 0));
-  const bool tma_ok = aligned16(A) && aligned16(B) && n <= static_cast<int64_t>(INT_MAX) - 2048;
+  // Box coordinates are 32-bit: the last chunk's boxes start below n + RS
+  // (RS <= 6144), so n leaves that much room below INT_MAX.
+  const bool tma_ok = aligned16(A) && aligned16(B) && n <= static_cast<int64_t>(INT_MAX) - 8192;
   int idx = -1;
   if (cm_a && cm_b && tma_ok) {
     const int wa = pow2_ceil(m), wb = pow2_ceil(k);
