@@ -180,8 +180,9 @@ tsm_status tsm_gram_f64(tsm_stream_t stream, int64_t n, int m, const double* A, 
  * Row-major operands (a_col = b_col = 1, a_row >= m, b_row >= k) take the
  * tsm_gemm_tn_f64 path.  Column-major operands (a_row = b_row = 1: A stored
  * as the m x n row-major matrix A^T with pitch a_col >= n, B likewise) stream
- * through tensor maps when the bases are 16-byte aligned and the pitches even
- * (values of r contiguous, columns zero-padded to the kernel's capacity);
+ * through tensor maps when the bases are 16-byte aligned, the pitches even and
+ * n <= 2^31 - 8193 (values of r contiguous, columns zero-padded to the
+ * kernel's capacity);
  * FP64 tensor cores when the widths rounded up to powers of two multiply to
  * more than 64.  Any other layout (mixed, odd pitches, unaligned) runs a
  * register-tile kernel with strided loads: correct, not tuned.  No
