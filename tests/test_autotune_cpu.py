@@ -1,0 +1,84 @@
+"""Host logic of the autotuner (no GPU): which variants are candidates for a
+shape, which candidates go to the interleaved refinement, how the winner is
+decided and how a partial re-tune merges into an earlier table; and that the
+committed tuned table names, for every shape, a variant that accepts it."""
+import json
+import os
+
+from tests.conftest import ROOT
+
+
+def test_candidates_follow_widths_and_dtype():
+    from tsm_benchmark_b200 import variants
+    from tsm_benchmark_b200.autotune import candidates
+    vs = variants()
+    for m, k in [(8, 8), (3, 5), (1, 64), (64, 64), (16, 16)]:
+        got = candidates(vs, m, k)
+        assert got, (m, k)
+        for v in got:
+            assert v["dtype"] == "f64" and not v["gram"], v["name"]
+            if v["exact"]:
+                assert (v["wa"], v["wb"]) == (m, k), v["name"]
+            else:
+                assert m <= v["wa"] and k <= v["wb"], v["name"]
+        names = {v["name"] for v in got}
+        # every exact variant of the pair, none of another width pair
+        exact = {v["name"] for v in vs if v["exact"] and v["dtype"] == "f64" and not v["gram"]
+                 and (v["wa"], v["wb"]) == (m, k)}
+        assert exact <= names
+    # capacities at most twice the smallest power of two per side: 3 x 5 takes
+    # 4..8 x 8..16, never 64-wide capacity kernels
+    for v in candidates(vs, 3, 5):
+        assert not v["exact"] and v["wa"] in (4, 8) and v["wb"] in (8, 16), v["name"]
+    assert all(v["dtype"] == "f32" for v in candidates(vs, 16, 16, dtype="f32"))
+
+
+def test_refinement_set_and_median_winner():
+    from tsm_benchmark_b200.autotune import median_winner, refinement_set
+    row = {"a": {"ms": 1.00, "ok": True}, "b": {"ms": 1.04, "ok": True}, "c": {"ms": 1.049, "ok": True},
+           "d": {"ms": 1.03, "ok": True}, "e": {"ms": 0.50, "ok": False}, "f": {"ms": 1.20, "ok": True}}
+    # the wrong result is never a candidate, however fast; at most three, within 5 %
+    assert refinement_set(row) == ["a", "d", "b"]
+    assert refinement_set({"x": {"ms": 1.0, "ok": True}, "y": {"ms": 1.06, "ok": True}}) == ["x"]
+    assert refinement_set({"x": {"ms": 1.0, "ok": False}}) == []
+    assert refinement_set({}) == []
+    # decided by the median, not by the single best sample
+    win, med = median_winner({"a": [1.00, 1.30, 1.31], "b": [1.10, 1.11, 1.12]})
+    assert win == "b" and med["a"] == 1.30
+    win, _ = median_winner({"a": [1.0, 2.0], "b": [1.5, 1.5]})
+    assert win == "a"  # equal medians: the first listed
+
+
+def test_merge_keeps_other_pairs():
+    from tsm_benchmark_b200.autotune import merge_results
+    old = {"choices": [{"m": 8, "k": 8, "nmin": 0, "variant": "old8"},
+                       {"m": 8, "k": 8, "nmin": 8388608, "variant": "old8big"},
+                       {"m": 1, "k": 1, "nmin": 0, "variant": "old1"}],
+           "timings": {"8x8@32768": {"old8": {}}, "1x1@32768": {"old1": {}}}}
+    res = {"device": "d", "choices": [{"m": 8, "k": 8, "nmin": 8388608, "variant": "new8big"},
+                                      {"m": 8, "k": 8, "nmin": 0, "variant": "new8"}],
+           "timings": {"8x8@67108864": {"new8big": {}}}}
+    out = merge_results(old, res, [(8, 8)])
+    assert [c["variant"] for c in out["choices"]] == ["old1", "new8", "new8big"]
+    assert set(out["timings"]) == {"1x1@32768", "8x8@67108864"}  # the re-tuned pair's old timings go
+    assert out["device"] == "d" and res["choices"][0]["variant"] == "new8big"  # inputs untouched
+
+
+def test_committed_tuned_table_is_consistent():
+    from tsm_benchmark_b200 import variants
+    from tsm_benchmark_b200.autotune import BUCKETS, candidates
+    with open(os.path.join(ROOT, "tsm_benchmark_b200", "tuned.json")) as f:
+        doc = json.load(f)
+    vs = variants()
+    seen = set()
+    nmins = {b[0] for b in BUCKETS}
+    for c in doc["choices"]:
+        m, k, nmin = int(c["m"]), int(c["k"]), int(c["nmin"])
+        assert (m, k, nmin) not in seen, c
+        seen.add((m, k, nmin))
+        assert nmin in nmins, c
+        assert c["variant"] in {v["name"] for v in candidates(vs, m, k)}, c
+    # every sweep shape has an entry for the headline bucket
+    from tsm_benchmark_b200.autotune import SWEEP_PAIRS
+    for m, k in SWEEP_PAIRS:
+        assert (m, k, BUCKETS[-1][0]) in seen, (m, k)

@@ -63,6 +63,35 @@ def candidates(variants: list[dict], m: int, k: int, dtype: str = "f64") -> list
     return out
 
 
+def refinement_set(row: dict, within: float = 1.05, top_n: int = 3) -> list[str]:
+    """Names of the fastest correct candidates of one shape, fastest first:
+    at most `top_n`, each within `within` times the fastest single timing.
+    `row` maps a variant name to {"ms": ..., "ok": ...}."""
+    top = sorted((r["ms"], name) for name, r in row.items() if r["ok"])
+    return [name for ms_, name in top[:top_n] if ms_ <= top[0][0] * within] if top else []
+
+
+def median_winner(samples: dict) -> tuple[str, dict]:
+    """The candidate with the smallest median over its interleaved timings
+    (ties go to the one listed first), and every candidate's median."""
+    med = {name: statistics.median(t) for name, t in samples.items()}
+    return min(med, key=med.get), med
+
+
+def merge_results(old: dict, res: dict, pairs) -> dict:
+    """`res` (a tuning of `pairs`) with the other pairs' choices and timings
+    of an earlier result `old` kept; choices sorted by (m, k, nmin)."""
+    tuned = {(int(m), int(k)) for m, k in pairs}
+    out = dict(res)
+    out["choices"] = [c for c in old.get("choices", []) if (int(c["m"]), int(c["k"])) not in tuned] + \
+        list(res["choices"])
+    out["choices"].sort(key=lambda c: (int(c["m"]), int(c["k"]), int(c.get("nmin", 0))))
+    kept = {key: val for key, val in old.get("timings", {}).items()
+            if tuple(int(x) for x in key.split("@")[0].split("x")) not in tuned}
+    out["timings"] = {**kept, **res["timings"]}
+    return out
+
+
 def time_variant(call, reps: int, warmup: int = 3) -> float:
     import torch
     for _ in range(warmup):
@@ -118,8 +147,7 @@ def tune(pairs, buckets=BUCKETS, reps_time_ms: float = 150.0, verbose: bool = Tr
             # interleaved rounds (A B C A B C ...), decided by the median --
             # single timings of near-equal kernels differ by a few percent
             # from run to run, more than the kernels do.
-            top = sorted((r["ms"], name) for name, r in row.items() if r["ok"])
-            top = [name for ms_, name in top[:3] if ms_ <= top[0][0] * 1.05] if top else []
+            top = refinement_set(row)
             if len(top) > 1:
                 idx = {v["name"]: v["index"] for v in vs}
                 reps = max(3, min(100, int(reps_time_ms / 3 / max(row[top[0]]["ms"], 1e-3))))
@@ -128,8 +156,7 @@ def tune(pairs, buckets=BUCKETS, reps_time_ms: float = 150.0, verbose: bool = Tr
                     for name in top:
                         call = lambda: tsmttsm(A, B, C, variant=idx[name])  # noqa: E731
                         samples[name].append(time_variant(call, reps, warmup=1))
-                med = {name: statistics.median(t) for name, t in samples.items()}
-                win = min(med, key=med.get)
+                win, med = median_winner(samples)
                 for name in top:
                     row[name]["median_ms_interleaved"] = round(med[name], 5)
                 best = (win, med[win], 8 * n * (m + k) / (med[win] * 1e-3) / 1e9)
@@ -162,13 +189,7 @@ def main(argv=None) -> int:
     res = tune(pairs, reps_time_ms=args.budget_ms)
     if args.merge and os.path.exists(args.out):
         with open(args.out) as f:
-            old = json.load(f)
-        tuned = {(int(m), int(k)) for m, k in pairs}
-        res["choices"] = [c for c in old.get("choices", []) if (int(c["m"]), int(c["k"])) not in tuned] + res["choices"]
-        res["choices"].sort(key=lambda c: (int(c["m"]), int(c["k"]), int(c.get("nmin", 0))))
-        kept = {key: val for key, val in old.get("timings", {}).items()
-                if tuple(int(x) for x in key.split("@")[0].split("x")) not in tuned}
-        res["timings"] = {**kept, **res["timings"]}
+            res = merge_results(json.load(f), res, pairs)
     with open(args.out, "w") as f:
         json.dump(res, f, indent=1)
         f.write("\n")
