@@ -502,7 +502,6 @@ def main() -> int:
     cs = float(C.sum()) if world == 1 else None
     bound = 4 * math.sqrt(HEAD_N) * 2.0**-53 * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B)) * 8
     checksum_ok = (cs is None) or abs(cs - chk) <= bound
-    dev_err = tsm.workspace_status(dev) if False else 0
     bits = ctypes.c_uint(0)
     lib.tsm_workspace_check(sh, ws.data_ptr(), ctypes.byref(bits))
     dev_err = int(bits.value)
@@ -558,9 +557,11 @@ def main() -> int:
                              "frac_roof": round(max(t_hbm, t_fp64) / (ms * 1e-3), 4),
                              "variant": tsm.variants()[vi]["name"] if vi >= 0 else None})
 
-    # ---------------- e2e through the C ABI from pinned host buffers
+    # ---------------- e2e through the C ABI from pinned host buffers: every
+    # rank copies its rows in, computes, joins the cross-rank sum (N > 1) and
+    # copies C out; max over ranks, bytes of the whole job.
     e2e = None
-    if world == 1 and args.e2e_steps > 0:
+    if args.e2e_steps > 0:
         Ah = torch.empty((HEAD_N, HEAD_M), dtype=torch.float64, pin_memory=True)
         Bh = torch.empty((HEAD_N, HEAD_K), dtype=torch.float64, pin_memory=True)
         Ah.copy_(A, non_blocking=False)
@@ -570,10 +571,12 @@ def main() -> int:
         def e2e_step():
             A.copy_(Ah, non_blocking=True)
             B.copy_(Bh, non_blocking=True)
-            call(A, B, C, HEAD_N, HEAD_M, HEAD_K)
+            step()
             Ch.copy_(C, non_blocking=True)
 
         e2e_step()
+        torch.cuda.synchronize()
+        barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -582,9 +585,16 @@ def main() -> int:
             e2e_step()
         e1.record(stream)
         torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.e2e_steps
-        e2e = {"value": bytes_step / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms,
-               "h2d_bytes_per_step": Ah.numel() * 8 + Bh.numel() * 8, "d2h_bytes_per_step": Ch.numel() * 8}
+        if world > 1:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        e2e = {"value": bytes_step * world / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms,
+               "h2d_bytes_per_step": (Ah.numel() * 8 + Bh.numel() * 8) * world,
+               "d2h_bytes_per_step": Ch.numel() * 8 * world}
         del Ah, Bh
 
     # ---------------- the precision, batching and differentiation forms
