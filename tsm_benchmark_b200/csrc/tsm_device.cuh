@@ -1,6 +1,6 @@
 // tsm_device.cuh -- device-side building blocks for the sm_100a kernels:
 // shared-memory addresses, mbarriers with bounded waits, 1-D TMA bulk copies
-// and 2-D tiled TMA loads (no multicast), tcgen05 helpers and the global
+// and 2-D tiled TMA loads into the issuing CTA only, tcgen05 helpers and the global
 // timer.
 //
 // Every wait here is bounded: after kWaitLimitNs of wall time the wait gives
@@ -101,7 +101,7 @@ __device__ __forceinline__ void bulk_g2s_evict_first(void* dst, const void* src,
       : "memory");
 }
 
-// 2-D tiled TMA load (no multicast) of the box at element coordinates
+// 2-D tiled TMA load, into this CTA alone, of the box at element coordinates
 // (x, y) of `tmap` into this CTA's shared memory, completing the box's bytes
 // on `bar`.  x * element size must be a multiple of 16 bytes; rows y beyond
 // the tensor are filled with zeros.  `tmap` is the generic address of a
