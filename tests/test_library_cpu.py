@@ -79,7 +79,9 @@ def test_python_layer_rejects_cpu_tensors():
 def test_c_abi_rejects_bad_arguments_before_any_cuda_call():
     """Argument checks that return before the first CUDA runtime call, so they
     run without a GPU: shapes, strides, part counts, pitches, alignment and
-    the 32-bit row limit of the tensor-map kernels.  The fake device
+    the 32-bit row limit of the tensor-map kernels, for every entry point
+    (plain, FP32, Gram, allocation-free, strided, split, TSMM, backward,
+    block orthogonalisation, batched, self-test, fill).  The fake device
     addresses are never dereferenced."""
     import ctypes
     from tsm_benchmark_b200 import _capi
@@ -110,6 +112,30 @@ def test_c_abi_rejects_bad_arguments_before_any_cuda_call():
     assert lib.tsm_gemm_tn_f32_split_bf16(None, 10, 8, 8, P, 16, P, 8, P, 8, 0, 3, P, 1 << 20) == UNSUPPORTED
     assert lib.tsm_gemm_tn_f32_split_bf16(None, 10, 8, 8, Q, 8, P, 8, P, 8, 0, 3, P, 1 << 20) == UNSUPPORTED
     assert lib.tsm_gemm_tn_f32_split_bf16(None, big, 8, 8, P, 8, P, 8, P, 8, 0, 2, P, 1 << 20) == UNSUPPORTED
+    # FP32 storage, Gram, allocation-free: the same shape checks as FP64
+    assert lib.tsm_gemm_tn_f32(None, 10, 8, 65, P, 8, P, 65, P, 65, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_f32(None, -1, 8, 8, P, 8, P, 8, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gram_f64(None, 10, 8, P, 7, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gram_f64(None, 10, 8, None, 8, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_f64_noalloc(None, 10, 8, 8, P, 8, P, 8, P, 7, 0) == INVALID
+    assert lib.tsm_gemm_tn_f64_noalloc(None, 10, 8, 8, P, 8, None, 8, P, 8, 0) == INVALID
+    # TSMM Y = X W: workspace first, then widths, pitches and pointers
+    assert lib.tsm_tsmm_f64(None, 10, 8, 8, P, 8, P, 8, 1, P, 8, 0, None, 0) == WORKSPACE
+    assert lib.tsm_tsmm_f64(None, 10, 8, 8, P, 8, P, 8, 1, P, 8, 0, Q, 1 << 20) == WORKSPACE
+    assert lib.tsm_tsmm_f64(None, 10, 65, 8, P, 65, P, 8, 1, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_tsmm_f64(None, 10, 8, 8, P, 4, P, 8, 1, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_tsmm_f64(None, 10, 8, 8, P, 8, None, 8, 1, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_tsmm_f64(None, 10, 8, 8, P, 8, P, 8, 1, None, 8, 0, P, 1 << 20) == INVALID
+    # backward: dC required, widths <= 64; with neither gradient asked for it does nothing
+    assert lib.tsm_gemm_tn_backward_f64(None, 10, 8, 8, P, 8, P, 8, None, 8, P, 8, P, 8, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_backward_f64(None, 10, 8, 65, P, 8, P, 65, P, 65, P, 8, P, 65, 0, P, 1 << 20) == INVALID
+    assert lib.tsm_gemm_tn_backward_f64(None, 10, 8, 8, P, 8, P, 8, P, 8, None, 8, None, 8, 0, P, 1 << 20) == 0
+    # block orthogonalisation: B is written, so it must be present
+    assert lib.tsm_block_orth_f64(None, 10, 8, 8, P, 8, None, 8, P, 8, P, 1 << 20) == INVALID
+    # batched: no plan, or a plan that was never initialised
+    assert lib.tsm_gemm_tn_batched_f64(None, None) == INVALID
+    assert lib.tsm_gemm_tn_batched_f64(None, ctypes.byref(_capi.BatchedPlan())) == INVALID
+    assert lib.tsm_batched_plan_init_f64(None, 1, None, P, 1 << 20, None) == INVALID
     # self-test and fill: workspace and count checks
     assert lib.tsm_selftest_wait_timeout(None, None, 0, 1000) == WORKSPACE
     assert lib.tsm_fill_uniform_f64(None, P, -1, 1, 0) == INVALID
