@@ -48,7 +48,6 @@ sycl::event accumulate_tn(sycl::queue& q, long long K, int M, int N, const T* A,
 
 // Index of the compiled variant called `name`, or -1 (use the default).
 inline int variant_by_name(const char* name) {
-  static thread_local std::string last;
   const int n = tsm_variant_count();
   for (int i = 0; i < n; ++i) {
     tsm_variant_info info;
