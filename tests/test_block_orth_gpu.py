@@ -3,7 +3,6 @@ update in one call, against the oracle; with orthonormal A the result is
 orthogonal to A's columns."""
 import numpy as np
 import pytest
-import torch
 
 from tests.test_plain_gpu import to_dev
 

@@ -4,7 +4,6 @@ workspace's error word, reported by tsm_workspace_check as
 TSM_ERROR_DEVICE_TIMEOUT, cleared, and the context keeps working."""
 import ctypes
 
-import numpy as np
 import pytest
 import torch
 

@@ -8,8 +8,6 @@ inside the library.  These tests drive it through the C ABI and compare it
 with tsm_gemm_tn_f64 (the workspace entry point) under the tolerance of the
 other parity tests.  This file is collected last on purpose.
 """
-import ctypes
-
 import numpy as np
 import pytest
 import torch
