@@ -67,13 +67,13 @@ def test_shard_rows_balanced():
             assert max(sizes) - min(sizes) <= 1
 
 
-def _batch_worker(rank: int, world: int, port: int, out_dir: str):
+def _batch_worker(rank: int, world: int, port: int, out_dir: str, count: int = 37):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     import datetime
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     from tsm_benchmark_b200.distributed import batched_sharded, shard_problems
-    shapes = _batch_shapes()
+    shapes = _batch_shapes(count)
     owned = shard_problems([8 * n * (m + k) for n, m, k in shapes], world)[rank]
     As, Bs = [], []
     for i in owned:
@@ -85,11 +85,11 @@ def _batch_worker(rank: int, world: int, port: int, out_dir: str):
     dist.destroy_process_group()
 
 
-def _batch_shapes():
+def _batch_shapes(count: int = 37):
     g = torch.Generator().manual_seed(11)
-    ns = torch.randint(1, 3000, (37,), generator=g).tolist()
-    ms = torch.randint(1, 9, (37,), generator=g).tolist()
-    ks = torch.randint(1, 9, (37,), generator=g).tolist()
+    ns = torch.randint(1, 3000, (count,), generator=g).tolist()
+    ms = torch.randint(1, 9, (count,), generator=g).tolist()
+    ks = torch.randint(1, 9, (count,), generator=g).tolist()
     return list(zip(ns, ms, ks))
 
 
@@ -100,14 +100,18 @@ def _batch_operands(i, shape):
             torch.rand((n, k), generator=g, dtype=torch.float64) * 2 - 1)
 
 
-def test_batched_sharded_by_problem_two_ranks(tmp_path):
+@pytest.mark.parametrize("count", [37, 1])
+def test_batched_sharded_by_problem_two_ranks(tmp_path, count):
     """Problems of a batch spread over ranks by cost; every rank ends with
-    every C_i, bit for bit the owner's result."""
+    every C_i, bit for bit the owner's result.  With one problem, rank 1
+    owns none and still joins the exchange."""
     world = 2
-    mp.start_processes(_batch_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+    mp.start_processes(_batch_worker, args=(world, _free_port(), str(tmp_path), count), nprocs=world,
                        start_method="spawn", join=True)
     res = [torch.load(tmp_path / f"batch{r}.pt") for r in range(world)]
-    shapes = _batch_shapes()
+    shapes = _batch_shapes(count)
+    if count == 1:
+        assert res[0]["owned"] == [0] and res[1]["owned"] == []
     owned = sorted(res[0]["owned"] + res[1]["owned"])
     assert owned == list(range(len(shapes))), "each problem owned by exactly one rank"
     for i, shape in enumerate(shapes):

@@ -92,7 +92,15 @@ def gather_problem_results(owned_C: Sequence[torch.Tensor], assignment: Sequence
     rank = dist.get_rank(group)
     sizes = [sum(shapes[i][0] * shapes[i][1] for i in owned) for owned in assignment]
     width = max(1, max(sizes))
-    dev = device if device is not None else (owned_C[0].device if owned_C else torch.device("cpu"))
+    if device is not None:
+        dev = device
+    elif owned_C:
+        dev = owned_C[0].device
+    elif dist.get_backend(group) == "nccl":
+        # a rank that owns no problem still joins the all-gather, from its GPU
+        dev = torch.device("cuda", torch.cuda.current_device())
+    else:
+        dev = torch.device("cpu")
     flat = torch.zeros(width, dtype=torch.float64, device=dev)
     off = 0
     for c, i in zip(owned_C, assignment[rank]):
