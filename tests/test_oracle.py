@@ -166,3 +166,13 @@ def test_tsmm_oracle(oracle_mod):
     W = rng.standard_normal((7, 5))
     assert np.allclose(oracle_mod.tsmm(X, W), X @ W, rtol=1e-13, atol=1e-13)
     assert np.allclose(oracle_mod.tsmm(X, W.T.copy(), transpose_w=True), X @ W, rtol=1e-13, atol=1e-13)
+
+
+def test_transpose_identity_and_empty(oracle_mod):
+    """naive(B, A) is naive(A, B) transposed bit for bit (the same products
+    summed over rows in the same order), and zero rows give a zero C."""
+    for n, m, k, seed in [(1, 1, 1, 1), (4099, 3, 5, 2), (30001, 8, 64, 3)]:
+        A, B = oracle_mod.operands(n, m, k, seed)
+        assert np.array_equal(oracle_mod.naive(B, A), oracle_mod.naive(A, B).T)
+    Z = oracle_mod.naive(np.zeros((0, 4)), np.zeros((0, 6)))
+    assert Z.shape == (4, 6) and not Z.any()
