@@ -409,8 +409,8 @@ def main() -> int:
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
-    ap.add_argument("--ref-rows", type=int, default=1 << 23)
-    ap.add_argument("--ref-budget", type=float, default=20.0)
+    ap.add_argument("--ref-rows", type=int, default=HEAD_N)
+    ap.add_argument("--ref-budget", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -470,14 +470,16 @@ def main() -> int:
         if world > 1:
             tsmdist.reduce_partials_(C)
 
-    # ---------------- headline: warmup, then K timed steps
+    # ---------------- headline: warmup, then K timed steps.  The clock
+    # sampler starts (and takes its start-up pause) before the warm-up, so
+    # the timed steps follow the warm-up with the GPU already at speed.
+    sampler = ClockSampler(local)
+    sampler.start()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
@@ -607,8 +609,11 @@ def main() -> int:
     # ---------------- CPU baseline (rank 0, N = 1)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        res = reference_cpu(args.ref_rows, steps=50, warmup=1, budget_s=args.ref_budget)
+        res = reference_cpu(args.ref_rows, steps=50, warmup=1, budget_s=20.0)
         cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample", "naive_single_core")}
+        # the same kernel on 1/8 of the rows: GB/s does not depend on n
+        small = reference_cpu(max(1, args.ref_rows // 8), steps=20, warmup=1, budget_s=5.0)
+        cpu["at_eighth_rows"] = {k: small[k] for k in ("value", "unit", "sample")}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -618,10 +623,44 @@ def main() -> int:
                 "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks, "by_width": by_width,
                 "fp64_peak": fp64_peak,
                 "checksum_ok": checksum_ok, "device_error_bits": dev_err, "forms": forms_out}
+        # the sweep, compactly, inside the roofline object: shape -> GB/s,
+        # binding roof and fraction of it
+        roofline["by_width"] = [{"shape": f"{r['n'].bit_length() - 1}:{r['m']}x{r['k']}", "GB/s": r["GB/s"],
+                                 "bound": r["bound"], "frac_roof": r["frac_roof"]} for r in by_width]
         print(json.dumps(line), flush=True)
+        print(summary(line), file=sys.stderr, flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def summary(line: dict) -> str:
+    """A short human-readable digest of the JSON line (stderr)."""
+    out = [f"headline {line['value']:.1f} GB/s ({line['ms_per_step']:.4f} ms/step), kernel alone "
+           f"{line['roofline']['achieved']:.1f} GB/s = {line['roofline']['frac']:.3f} of {line['roofline']['peak']} "
+           f"({line['roofline']['peak_source']})"]
+    if line.get("e2e"):
+        out.append(f"e2e {line['e2e']['value']:.2f} GB/s")
+    for r in line.get("by_width") or []:
+        out.append(f"  n=2^{r['n'].bit_length() - 1} {r['m']}x{r['k']}: {r['GB/s']} GB/s, {r['GFLOP/s']} GFLOP/s, "
+                   f"{r['bound']} {r['frac_roof']}, {r['variant']}")
+    f = line.get("forms") or {}
+    for key in ("split_tf32", "split_bf16x2", "split_bf16x3"):
+        if key in f:
+            x = f[key]
+            out.append(f"  {key}: {x['ms']} ms vs FP64 {x['fp64_ms']} ms ({x['speedup_vs_fp64']}x; sustained "
+                       f"{x['sustained_300_calls']['speedup_vs_fp64']}x), err {x['err_normwise_rel']:.2e}")
+    if "batched" in f:
+        x = f["batched"]
+        out.append(f"  batched: {x['ms']} ms, {x['GB/s']} GB/s, {x['speedup_vs_fp64_plain']}x per-problem launches")
+    for key in ("autograd_f64", "autograd_f32"):
+        if key in f:
+            x = f[key]
+            out.append(f"  {key}: fwd {x['fwd_ms']} ms, bwd {x['bwd_ms']} ms ({x['bwd_over_fwd']}x)")
+    if line.get("cpu_baseline"):
+        c = line["cpu_baseline"]
+        out.append(f"cpu baseline ({c['kind']}, {c['cores']} cores): {c['value']:.3f} GB/s; {c['sample']}")
+    return "\n".join(out)
 
 
 if __name__ == "__main__":

@@ -209,9 +209,21 @@ tsm_status tsm_gemm_tn_strided_f64(tsm_stream_t stream, int64_t n, int m, int k,
  * TSM_ERROR_WORKSPACE and launch nothing.  All calls share the array: calls
  * that overlap on the GPU race and must be serialised by the caller.  The
  * first call on each device looks up the array's device address; make it
- * before any stream capture.  Device error bits are not reported. */
+ * before any stream capture.  The address, like all per-device state of the
+ * library, does not survive cudaDeviceReset.  A kernel that gives up a
+ * bounded wait records it in the array's error word: read it with
+ * tsm_noalloc_check. */
 tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
                                    const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate);
+
+/* Reads and clears the error word of tsm_gemm_tn_f64_noalloc's built-in
+ * scratch on the current device (synchronises `stream`), as
+ * tsm_workspace_check does for a caller's workspace: *bits != 0 means a
+ * kernel of an earlier no-allocation call gave up a bounded wait and its C
+ * is not valid; the call then returns TSM_ERROR_DEVICE_TIMEOUT.  The word
+ * stays set until read.  Allocates nothing.  No counterpart in the reference
+ * (it has no failure detection). */
+tsm_status tsm_noalloc_check(tsm_stream_t stream, unsigned* bits);
 
 /* Tall-skinny times small (TSMM): Y (n x q) = X (n x p) * W (beta = 0) or
  * Y += X * W (beta = 1), FP64 or FP32, 1 <= p, q <= 64.  W is read as

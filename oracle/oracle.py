@@ -29,9 +29,27 @@ _lib = None
 _ref = None
 
 
+# The reference checkout whose sources oracle/Makefile compiles in place:
+# TSM_REFERENCE_DIR from the environment, else the read-only checkout the
+# project is built beside, when it is there (it is not on GPU hosts, which
+# use the libraries built where it is).
+REFERENCE_CHECKOUT = "/root/reference"
+
+
+def reference_dir() -> str | None:
+    d = os.environ.get("TSM_REFERENCE_DIR") or REFERENCE_CHECKOUT
+    return d if os.path.exists(os.path.join(d, "main.cc")) else None
+
+
+def make_args() -> list[str]:
+    """REF_DIR=<checkout> for the Makefiles, or nothing without a checkout."""
+    d = reference_dir()
+    return [f"REF_DIR={d}"] if d else []
+
+
 def build() -> None:
     """Runs oracle/Makefile (the reference part only where its sources exist)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, *make_args()], check=True)
 
 
 def lib() -> ctypes.CDLL:
@@ -52,6 +70,11 @@ def lib() -> ctypes.CDLL:
         L.tsm_oracle_v4_omp.restype = I
         L.tsm_oracle_num_threads.restype = I
         L.tsm_oracle_tsmm_f64.argtypes = [I64, I, I, P, I64, P, I64, I64, P, I64, I]
+        L.tsm_oracle_dot2_acc.argtypes = [I64, I, I, P, I64, P, I64, I, P, P, P, P]
+        L.tsm_oracle_dot2_acc.restype = I
+        L.tsm_oracle_dot2_uniform.argtypes = [I64, I64, I, I, ctypes.c_uint64, P, P, P, P]
+        L.tsm_oracle_dot2_uniform.restype = I
+        L.tsm_oracle_force_split.argtypes = [I]
         _lib = L
     return _lib
 
@@ -171,3 +194,59 @@ def tsmm(X: np.ndarray, W: np.ndarray, transpose_w: bool = False) -> np.ndarray:
     Y = np.zeros((n, q))
     lib().tsm_oracle_tsmm_f64(n, p, q, _p(X), ldx, _p(Wc), w_row, w_col, _p(Y), q, 0)
     return Y
+
+
+class Dot2Stream:
+    """Compensated A^T B accumulated over row chunks (tsm_oracle_dot2_acc /
+    tsm_oracle_dot2_uniform): the full-size checks feed it host chunks or let
+    it generate the counter-based uniform operands itself, so no operand is
+    ever held whole.  ``result()`` gives C rounded to FP64, the Frobenius
+    norms of A and B, the normwise bound 4 sqrt(n) 2^-53 ||A||_F ||B||_F and,
+    with ``with_abs``, sum_r |a_ri| |b_rj| per entry."""
+
+    def __init__(self, m: int, k: int, with_abs: bool = False):
+        self.m, self.k, self.rows = m, k, 0
+        self.S = np.zeros(m * k)
+        self.E = np.zeros(m * k)
+        self.nrm = np.zeros(2)
+        self.absC = np.zeros(m * k) if with_abs else None
+
+    def _abs(self):
+        return _p(self.absC) if self.absC is not None else None
+
+    def add(self, A: np.ndarray, B: np.ndarray) -> None:
+        n, m, lda = _rows(A)
+        n2, k, ldb = _rows(B)
+        assert (n, m, k) == (n2, self.m, self.k) and A.dtype == B.dtype
+        f32 = 1 if A.dtype == np.float32 else 0
+        assert f32 or A.dtype == np.float64
+        rc = lib().tsm_oracle_dot2_acc(n, m, k, _p(A), lda, _p(B), ldb, f32, _p(self.S), _p(self.E), _p(self.nrm),
+                                       self._abs())
+        if rc != 0:
+            raise MemoryError("oracle: host buffers")
+        self.rows += n
+
+    def add_uniform(self, seed: int, row0: int, rows: int) -> None:
+        """Rows [row0, row0 + rows) of operands(n, m, k, seed)'s values."""
+        rc = lib().tsm_oracle_dot2_uniform(row0, rows, self.m, self.k, seed, _p(self.S), _p(self.E), _p(self.nrm),
+                                           self._abs())
+        if rc != 0:
+            raise MemoryError("oracle: host buffers")
+        self.rows += rows
+
+    def result(self) -> dict:
+        C = (self.S + self.E).reshape(self.m, self.k)
+        na, nb = float(np.sqrt(self.nrm[0])), float(np.sqrt(self.nrm[1]))
+        out = dict(C=C, normA=na, normB=nb, rows=self.rows,
+                   bound=4.0 * np.sqrt(float(self.rows)) * 2.0**-53 * na * nb)
+        if self.absC is not None:
+            out["absC"] = self.absC.reshape(self.m, self.k).copy()
+        return out
+
+
+def dot2_uniform(n: int, m: int, k: int, seed: int, with_abs: bool = False) -> dict:
+    """Dot2Stream over all n rows of operands(n, m, k, seed), generated on
+    the host as it goes."""
+    d = Dot2Stream(m, k, with_abs)
+    d.add_uniform(seed, 0, n)
+    return d.result()

@@ -289,3 +289,225 @@ EXPORT void tsm_oracle_tsmm_f64(int64_t n, int p, int q, const double* X,
       Y[r * ldy + b] = beta ? Y[r * ldy + b] + acc : acc;
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Streaming compensated product for the full-size checks.                   */
+/* ------------------------------------------------------------------------ */
+
+/* The full-size configurations (up to 2^26 rows, 32 GiB per operand) are
+ * checked against a compensated product (Dot2, Ogita, Rump and Oishi 2005,
+ * as tsm_oracle_dot2_f64 above) computed over row blocks, so that the host
+ * never holds a whole operand.  Its result is within about one rounding of
+ * the exact A^T B, so the comparison measures the tested kernel's own error
+ * against the normwise bound 4 sqrt(n) 2^-53 ||A||_F ||B||_F.
+ *
+ * State carried across calls (the caller zero-fills it first):
+ *   S[m*k], E[m*k]  -- the double-double sum, value S + E;
+ *   nrm[2]          -- sum of A's squares, sum of B's squares;
+ *   absC[m*k]       -- optional (NULL to skip): sum_r |a_ri| |b_rj|, the
+ *                      entries' own condition scale.
+ * Each call splits its rows over the OpenMP threads (contiguous ranges), each
+ * thread keeps its own double-double sums, and the threads' sums are merged
+ * in thread order with the same error-free additions. */
+
+#define DOT2_BLOCK 256
+
+static inline void dot2_merge(double* s, double* e, double hi, double lo) {
+  const double t = *s + hi;
+  const double z = t - *s;
+  const double es = (*s - (t - z)) + (hi - z);
+  *s = t;
+  *e += es + lo;
+}
+
+/* One block of rows, both operands as doubles with pitches m and k.  The
+ * product's rounding error comes from an FMA where the host has one; the
+ * other body splits the factors (Veltkamp/Dekker) -- both exact, since the
+ * file is compiled with -ffp-contract=off. */
+__attribute__((target("avx2,fma"))) static void dot2_rows_fma(
+    int64_t rows, int m, int k, const double* a, const double* b, double* s, double* c) {
+  for (int64_t r = 0; r < rows; ++r) {
+    const double* ar = a + r * m;
+    const double* br = b + r * k;
+    for (int i = 0; i < m; ++i) {
+      const double ai = ar[i];
+      double* si = s + (int64_t)i * k;
+      double* ci = c + (int64_t)i * k;
+#pragma omp simd
+      for (int j = 0; j < k; ++j) {
+        const double p = ai * br[j];
+        const double ep = __builtin_fma(ai, br[j], -p);
+        const double t = si[j] + p;
+        const double z = t - si[j];
+        const double es = (si[j] - (t - z)) + (p - z);
+        si[j] = t;
+        ci[j] += es + ep;
+      }
+    }
+  }
+}
+
+static void dot2_rows_split(int64_t rows, int m, int k, const double* a, const double* b, double* s,
+                            double* c) {
+  const double kSplit = 134217729.0; /* 2^27 + 1 */
+  for (int64_t r = 0; r < rows; ++r) {
+    const double* ar = a + r * m;
+    const double* br = b + r * k;
+    for (int i = 0; i < m; ++i) {
+      const double ai = ar[i];
+      const double ga = kSplit * ai, ah = ga - (ga - ai), al = ai - ah;
+      double* si = s + (int64_t)i * k;
+      double* ci = c + (int64_t)i * k;
+#pragma omp simd
+      for (int j = 0; j < k; ++j) {
+        const double bj = br[j];
+        const double gb = kSplit * bj, bh = gb - (gb - bj), bl = bj - bh;
+        const double p = ai * bj;
+        const double ep = ((ah * bh - p) + ah * bl + al * bh) + al * bl;
+        const double t = si[j] + p;
+        const double z = t - si[j];
+        const double es = (si[j] - (t - z)) + (p - z);
+        si[j] = t;
+        ci[j] += es + ep;
+      }
+    }
+  }
+}
+
+static int g_force_split = 0;
+
+static int host_has_fma(void) {
+  static int cached = -1;
+  if (cached < 0) cached = __builtin_cpu_supports("avx2") && __builtin_cpu_supports("fma");
+  return cached && !g_force_split;
+}
+
+/* Makes the streaming product use the factor-splitting body even where the
+ * host has an FMA (the CPU tests check both bodies against each other). */
+EXPORT void tsm_oracle_force_split(int on) { g_force_split = on; }
+
+/* Where a block's values come from: host arrays (FP64 or FP32, row pitches
+ * lda, ldb), or the counter-based uniform generator (A = stream 0, B =
+ * stream 1 under `seed`, contiguous: element (r, i) of A is value r*m + i). */
+typedef struct {
+  const void* A;
+  const void* B;
+  int64_t lda, ldb;
+  int f32;
+  int generate;
+  uint64_t seed;
+  int64_t row0; /* global index of row 0 of this call (generator) */
+} dot2_source;
+
+static void dot2_load(const dot2_source* src, int m, int k, int64_t r, int64_t rows, double* a,
+                      double* b) {
+  if (src->generate) {
+    for (int64_t q = 0; q < rows * m; ++q) {
+      const uint64_t idx = (uint64_t)((src->row0 + r) * m) + (uint64_t)q;
+      a[q] = 2.0 * ((double)(splitmix64_at(src->seed, 0, idx) >> 11) * 0x1.0p-53) - 1.0;
+    }
+    for (int64_t q = 0; q < rows * k; ++q) {
+      const uint64_t idx = (uint64_t)((src->row0 + r) * k) + (uint64_t)q;
+      b[q] = 2.0 * ((double)(splitmix64_at(src->seed, 1, idx) >> 11) * 0x1.0p-53) - 1.0;
+    }
+    return;
+  }
+  for (int64_t q = 0; q < rows; ++q) {
+    for (int i = 0; i < m; ++i)
+      a[q * m + i] = src->f32 ? (double)((const float*)src->A)[(r + q) * src->lda + i]
+                              : ((const double*)src->A)[(r + q) * src->lda + i];
+    for (int j = 0; j < k; ++j)
+      b[q * k + j] = src->f32 ? (double)((const float*)src->B)[(r + q) * src->ldb + j]
+                              : ((const double*)src->B)[(r + q) * src->ldb + j];
+  }
+}
+
+static int dot2_stream(const dot2_source* src, int64_t rows, int m, int k, double* S, double* E,
+                       double* nrm, double* absC) {
+  const int64_t mk = (int64_t)m * k;
+  int nt = 1;
+#ifdef _OPENMP
+  nt = omp_get_max_threads();
+#endif
+  /* per thread: s, c (and abs) sums, two norms */
+  const int64_t stride = 3 * mk + 2;
+  double* part = (double*)calloc((size_t)nt * (size_t)stride, sizeof(double));
+  if (!part) return -1;
+  int failed = 0;
+  const int fma_ok = host_has_fma();
+#pragma omp parallel num_threads(nt)
+  {
+    int t = 0, T = 1;
+#ifdef _OPENMP
+    t = omp_get_thread_num();
+    T = omp_get_num_threads();
+#endif
+    const int64_t r0 = rows * t / T, r1 = rows * (t + 1) / T;
+    double* s = part + (int64_t)t * stride;
+    double* c = s + mk;
+    double* ab = c + mk;
+    double* nr = ab + mk;
+    double* a = (double*)malloc(sizeof(double) * DOT2_BLOCK * (size_t)m);
+    double* b = (double*)malloc(sizeof(double) * DOT2_BLOCK * (size_t)k);
+    if (!a || !b) {
+#pragma omp atomic write
+      failed = 1;
+    } else {
+      for (int64_t r = r0; r < r1; r += DOT2_BLOCK) {
+        const int64_t nb = (r1 - r < DOT2_BLOCK) ? r1 - r : DOT2_BLOCK;
+        dot2_load(src, m, k, r, nb, a, b);
+        if (fma_ok)
+          dot2_rows_fma(nb, m, k, a, b, s, c);
+        else
+          dot2_rows_split(nb, m, k, a, b, s, c);
+        for (int64_t q = 0; q < nb * m; ++q) nr[0] += a[q] * a[q];
+        for (int64_t q = 0; q < nb * k; ++q) nr[1] += b[q] * b[q];
+        if (absC) {
+          for (int64_t q = 0; q < nb; ++q)
+            for (int i = 0; i < m; ++i) {
+              const double ai = fabs(a[q * m + i]);
+              for (int j = 0; j < k; ++j) ab[(int64_t)i * k + j] += ai * fabs(b[q * k + j]);
+            }
+        }
+      }
+    }
+    free(a);
+    free(b);
+  }
+  if (!failed) {
+    for (int t = 0; t < nt; ++t) {
+      const double* s = part + (int64_t)t * stride;
+      const double* c = s + mk;
+      const double* ab = c + mk;
+      const double* nr = ab + mk;
+      for (int64_t q = 0; q < mk; ++q) {
+        dot2_merge(&S[q], &E[q], s[q], c[q]);
+        if (absC) absC[q] += ab[q];
+      }
+      nrm[0] += nr[0];
+      nrm[1] += nr[1];
+    }
+  }
+  free(part);
+  return failed ? -1 : 0;
+}
+
+/* Adds one chunk of host rows (A: rows x m, pitch lda; B: rows x k, pitch
+ * ldb; FP64, or FP32 widened exactly when f32 != 0) into the state.
+ * Returns 0, or -1 when a buffer could not be allocated. */
+EXPORT int tsm_oracle_dot2_acc(int64_t rows, int m, int k, const void* A, int64_t lda, const void* B,
+                               int64_t ldb, int f32, double* S, double* E, double* nrm, double* absC) {
+  if (rows <= 0) return 0;
+  dot2_source src = {A, B, lda, ldb, f32, 0, 0, 0};
+  return dot2_stream(&src, rows, m, k, S, E, nrm, absC);
+}
+
+/* The same over the counter-based uniform operands of `seed` (A = stream 0,
+ * B = stream 1, contiguous, rows [row0, row0 + rows)): the values the
+ * library's device fill writes, generated block by block on the host. */
+EXPORT int tsm_oracle_dot2_uniform(int64_t row0, int64_t rows, int m, int k, uint64_t seed, double* S,
+                                   double* E, double* nrm, double* absC) {
+  if (rows <= 0) return 0;
+  dot2_source src = {NULL, NULL, 0, 0, 0, 1, seed, row0};
+  return dot2_stream(&src, rows, m, k, S, E, nrm, absC);
+}

@@ -176,3 +176,50 @@ def test_transpose_identity_and_empty(oracle_mod):
         assert np.array_equal(oracle_mod.naive(B, A), oracle_mod.naive(A, B).T)
     Z = oracle_mod.naive(np.zeros((0, 4)), np.zeros((0, 6)))
     assert Z.shape == (4, 6) and not Z.any()
+
+
+def test_streaming_dot2_is_correctly_rounded_and_chunk_invariant(oracle_mod):
+    """The full-size oracle (compensated product over row blocks): against
+    exact rational sums it rounds correctly; feeding the rows in chunks, or
+    letting it generate the counter-based operands itself, gives the same C;
+    the factor-splitting body (hosts without FMA) agrees with the FMA one."""
+    from fractions import Fraction
+    n, m, k = 2001, 3, 4
+    A, B = oracle_mod.operands(n, m, k, 7)
+    exact = np.array([[float(sum(Fraction(a) * Fraction(b) for a, b in zip(A[:, i], B[:, j])))
+                       for j in range(k)] for i in range(m)])
+    d = oracle_mod.Dot2Stream(m, k, with_abs=True)
+    d.add(A[:700], B[:700])
+    d.add(A[700:], B[700:])
+    r = d.result()
+    assert np.array_equal(r["C"], exact)
+    assert r["rows"] == n
+    assert np.allclose(r["absC"], np.abs(A).T @ np.abs(B), rtol=1e-13)
+    assert r["normA"] == pytest.approx(np.linalg.norm(A), rel=1e-13)
+    assert r["bound"] == pytest.approx(4 * np.sqrt(n) * 2.0**-53 * np.linalg.norm(A) * np.linalg.norm(B), rel=1e-12)
+    assert np.array_equal(oracle_mod.dot2_uniform(n, m, k, 7)["C"], exact)
+    g = oracle_mod.Dot2Stream(m, k)
+    g.add_uniform(7, 0, 1000)
+    g.add_uniform(7, 1000, n - 1000)
+    assert np.array_equal(g.result()["C"], exact)
+    oracle_mod.lib().tsm_oracle_force_split(1)
+    try:
+        assert np.array_equal(oracle_mod.dot2_uniform(n, m, k, 7)["C"], exact)
+    finally:
+        oracle_mod.lib().tsm_oracle_force_split(0)
+    # FP32 input is widened exactly
+    A32, B32 = A.astype(np.float32), B.astype(np.float32)
+    f = oracle_mod.Dot2Stream(m, k)
+    f.add(A32, B32)
+    assert np.array_equal(f.result()["C"], oracle_mod.dot2(A32.astype(np.float64), B32.astype(np.float64)))
+
+
+def test_streaming_dot2_decides_between_naive_and_blocked_sums(oracle_mod):
+    """At 2^20 rows the compensated result is closer to every entry than the
+    naive running sum (whose error grows with n), and the naive sum meets the
+    normwise bound measured against it."""
+    A, B = oracle_mod.operands(1 << 20, 4, 4, 11)
+    ref = oracle_mod.dot2_uniform(1 << 20, 4, 4, 11)
+    naive = oracle_mod.naive(A, B)
+    assert np.linalg.norm(naive - ref["C"]) <= ref["bound"]
+    assert np.all(np.abs(ref["C"] - oracle_mod.dot2(A, B)) <= np.spacing(np.abs(ref["C"])))

@@ -249,3 +249,36 @@ def test_every_fp32_exact_variant(gpu, oracle_mod):
             assert err <= bound + 1e-30, (v["name"], n, err, bound)
         ran += 1
     assert ran >= 21
+
+
+def test_side_stream_with_fresh_workspace_cache(gpu, oracle_mod, monkeypatch):
+    """A call on a caller-supplied stream creates its workspace ON that
+    stream: the zero-fill is ordered before the kernel even while the
+    current stream is busy.  The current stream is kept busy with a long
+    fill, and the products run on a side stream with an empty cache; the
+    batched plan is built and run on the side stream too."""
+    from tsm_benchmark_b200 import BatchedTSMTTSM, api, gram, tsmttsm, tsmttsm_split
+    monkeypatch.setattr(api, "_workspaces", {})
+    side = torch.cuda.Stream(gpu)
+    A, B = oracle_mod.operands(100003, 8, 16, 41)
+    A32, B32 = A.astype(np.float32), B.astype(np.float32)
+    dA, dB, dA32, dB32 = (to_dev(x, gpu) for x in (A, B, A32, B32))
+    busy = torch.empty(1 << 28, dtype=torch.float64, device=gpu)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        busy.fill_(1.0)  # ~2 GiB of writes queued on the current stream
+        with torch.cuda.stream(side):
+            C = tsmttsm(dA, dB, stream=side)
+            G = gram(dA, stream=side)
+            S = tsmttsm_split(dA32, dB32, stream=side)
+            bt = BatchedTSMTTSM([dA], [dB], stream=side)
+            Cb = bt.run(stream=side)[0]
+        side.synchronize()
+        assert_parity(oracle_mod, A, B, C, what="side stream")
+        assert_parity(oracle_mod, A, A, G, what="side stream gram")
+        assert_parity(oracle_mod, A, B, Cb, what="side stream batched")
+        ref32 = oracle_mod.naive(A32, B32)
+        assert np.linalg.norm(S.cpu().numpy() - ref32) <= 1e-6 * np.linalg.norm(ref32)
+        monkeypatch.setattr(api, "_workspaces", {})
+    torch.cuda.synchronize()
+    del busy

@@ -66,6 +66,43 @@ def test_noalloc_matches_workspace_entry_point(n, m, k):
     assert st == 0
     torch.cuda.synchronize()
     assert_close(2 * C_ref, C, "accumulate")
+    assert_no_device_error(lib, sh)
+
+
+def assert_no_device_error(lib, sh):
+    """No kernel of the calls above gave up a bounded wait: the scratch's
+    error word, read and cleared by tsm_noalloc_check, is zero."""
+    import ctypes
+    bits = ctypes.c_uint(0xFFFFFFFF)
+    st = lib.tsm_noalloc_check(sh, ctypes.byref(bits))
+    assert st == 0 and bits.value == 0, (st, bits.value)
+
+
+@pytest.mark.parametrize("n,m", [(1 << 20, 8), (100003, 16), (4099, 5), (20011, 32)])
+def test_noalloc_gram_route_when_b_is_a(n, m):
+    """B passed as A itself (same pointer, pitch and width) takes the Gram
+    kernels, which stream A once and write C exactly symmetric; the result
+    matches the workspace entry point's on the same request, twice."""
+    from tsm_benchmark_b200 import _capi
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    lib = _capi.load()
+    sh = int(torch.cuda.current_stream(dev).cuda_stream)
+    A, _ = operands(dev, n, m, 1, seed=n + m)
+    need = lib.tsm_gemm_tn_workspace_size(n, m, m)
+    ws = torch.zeros(need, dtype=torch.uint8, device=dev)
+    C_ref = torch.empty((m, m), dtype=torch.float64, device=dev)
+    st = lib.tsm_gemm_tn_f64(sh, n, m, m, A.data_ptr(), m, A.data_ptr(), m, C_ref.data_ptr(), m, 0,
+                             ws.data_ptr(), need)
+    assert st == 0, _capi.STATUS[st]
+    for call in range(2):
+        C = torch.full((m, m), float("nan"), dtype=torch.float64, device=dev)
+        st = lib.tsm_gemm_tn_f64_noalloc(sh, n, m, m, A.data_ptr(), m, A.data_ptr(), m, C.data_ptr(), m, 0)
+        assert st == 0, _capi.STATUS[st]
+        torch.cuda.synchronize()
+        assert_close(C_ref, C, f"Gram call {call + 1}, n={n} m={m}")
+        assert torch.equal(C, C.T)
+    assert_no_device_error(lib, sh)
 
 
 def test_noalloc_rejects_requests_beyond_its_scratch():

@@ -112,6 +112,7 @@ SIGNATURES = {
     "tsm_gemm_tn_batched_f64": (c_int, [c_void_p, ctypes.POINTER(BatchedPlan)]),
     "tsm_gemm_tn_f64_noalloc": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int]),
+    "tsm_noalloc_check": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint)]),
 }
 
 _lib = None

@@ -8,6 +8,7 @@ in other layouts (column-major ``X.T`` views included) go through
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import threading
 
@@ -19,19 +20,40 @@ _ws_lock = threading.Lock()
 _workspaces: dict[tuple[int, int], torch.Tensor] = {}
 
 
+def _stream(device: torch.device, stream: torch.cuda.Stream | None) -> torch.cuda.Stream:
+    return stream if stream is not None else torch.cuda.current_stream(device)
+
+
 def _stream_handle(device: torch.device, stream: torch.cuda.Stream | None) -> int:
-    s = stream if stream is not None else torch.cuda.current_stream(device)
-    return int(s.cuda_stream)
+    return int(_stream(device, stream).cuda_stream)
 
 
-def workspace(device: torch.device, nbytes: int, stream_handle: int) -> torch.Tensor:
+def _on_stream(device: torch.device, stream):
+    """Context in which torch allocates and launches on `stream` (a
+    torch.cuda.Stream or a raw cudaStream_t handle)."""
+    if isinstance(stream, torch.cuda.Stream):
+        return torch.cuda.stream(stream)
+    if torch.cuda.is_available():
+        return torch.cuda.stream(torch.cuda.ExternalStream(int(stream), device=device))
+    return contextlib.nullcontext()  # no device: only fake allocators reach here
+
+
+def workspace(device: torch.device, nbytes: int, stream) -> torch.Tensor:
     """A zero-initialised device workspace of at least `nbytes`, one per
-    (device, stream): calls on one stream are ordered, so they may share it."""
-    key = (device.index if device.index is not None else torch.cuda.current_device(), stream_handle)
+    (device, stream): calls on one stream are ordered, so they may share it.
+
+    `stream` is the torch.cuda.Stream (or raw handle) the kernels will run
+    on.  The buffer is allocated and zero-filled ON that stream, so the
+    zero-fill is ordered before the first launch that uses it, and the
+    caching allocator hands a replaced (smaller) buffer out again only to
+    later work on the same stream, after the launches that used it."""
+    handle = int(stream.cuda_stream) if isinstance(stream, torch.cuda.Stream) else int(stream)
+    key = (device.index if device.index is not None else torch.cuda.current_device(), handle)
     with _ws_lock:
         ws = _workspaces.get(key)
         if ws is None or ws.numel() < nbytes:
-            ws = torch.zeros(max(nbytes, 1 << 20), dtype=torch.uint8, device=device)
+            with _on_stream(device, stream):
+                ws = torch.zeros(max(nbytes, 1 << 20), dtype=torch.uint8, device=device)
             _workspaces[key] = ws
         return ws
 
@@ -104,11 +126,12 @@ def tsmttsm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = None, *, 
             raise ValueError(f"C must be {m}x{k}, got {tuple(C.shape)}")
     lib = _capi.load()
     with torch.cuda.device(A.device):
-        sh = _stream_handle(A.device, stream)
+        so = _stream(A.device, stream)
+        sh = int(so.cuda_stream)
         need = lib.tsm_gemm_tn_workspace_size(n, m, k)
         if need == 0:
             _capi.check(1, "tsm_gemm_tn_workspace_size")
-        ws = workspace(A.device, need, sh)
+        ws = workspace(A.device, need, so)
         if _row_major(A) and _row_major(B):
             st = getattr(lib, fn_name)(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
                                        _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel(), int(variant))
@@ -138,11 +161,12 @@ def gram(A: torch.Tensor, C: torch.Tensor | None = None, *, accumulate: bool = F
             raise ValueError(f"C must be {m}x{m}, got {tuple(C.shape)}")
     lib = _capi.load()
     with torch.cuda.device(A.device):
-        sh = _stream_handle(A.device, stream)
+        so = _stream(A.device, stream)
+        sh = int(so.cuda_stream)
         need = lib.tsm_gemm_tn_workspace_size(n, m, m)
         if need == 0:
             _capi.check(1, "tsm_gemm_tn_workspace_size")
-        ws = workspace(A.device, need, sh)
+        ws = workspace(A.device, need, so)
         st = lib.tsm_gram_f64(sh, n, m, A.data_ptr(), _ld(A), C.data_ptr(), _ld(C), 1 if accumulate else 0,
                               ws.data_ptr(), ws.numel())
         _capi.check(st, "tsm_gram_f64")
@@ -168,11 +192,12 @@ def block_orthogonalize(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None
             raise ValueError(f"C must be {m}x{k}, got {tuple(C.shape)}")
     lib = _capi.load()
     with torch.cuda.device(A.device):
-        sh = _stream_handle(A.device, stream)
+        so = _stream(A.device, stream)
+        sh = int(so.cuda_stream)
         need = lib.tsm_gemm_tn_workspace_size(n, m, k)
         if need == 0:
             _capi.check(1, "tsm_gemm_tn_workspace_size")
-        ws = workspace(A.device, need, sh)
+        ws = workspace(A.device, need, so)
         st = lib.tsm_block_orth_f64(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(), _ld(C),
                                     ws.data_ptr(), ws.numel())
         _capi.check(st, "tsm_block_orth_f64")
@@ -249,8 +274,9 @@ def tsmm(X: torch.Tensor, W: torch.Tensor, Y: torch.Tensor | None = None, *, tra
             raise ValueError(f"Y must be {n}x{q}, got {tuple(Y.shape)}")
     lib = _capi.load()
     with torch.cuda.device(X.device):
-        sh = _stream_handle(X.device, stream)
-        ws = workspace(X.device, 256, sh)
+        so = _stream(X.device, stream)
+        sh = int(so.cuda_stream)
+        ws = workspace(X.device, 256, so)
         st = getattr(lib, _TSMM[X.dtype])(sh, n, p, q, X.data_ptr(), _ld(X), W.data_ptr(), w_row, w_col,
                                            Y.data_ptr(), _ld(Y), 1 if accumulate else 0, ws.data_ptr(), ws.numel())
         _capi.check(st, _TSMM[X.dtype])
@@ -276,8 +302,9 @@ def tsmttsm_backward(A: torch.Tensor, B: torch.Tensor, dC: torch.Tensor, *, need
     dB = torch.empty((n, k), dtype=A.dtype, device=A.device) if need_dB else None
     lib = _capi.load()
     with torch.cuda.device(A.device):
-        sh = _stream_handle(A.device, stream)
-        ws = workspace(A.device, 256, sh)
+        so = _stream(A.device, stream)
+        sh = int(so.cuda_stream)
+        ws = workspace(A.device, 256, so)
         st = getattr(lib, _BWD[A.dtype])(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), dC.data_ptr(),
                                           k, dA.data_ptr() if dA is not None else None, m,
                                           dB.data_ptr() if dB is not None else None, k, 0, ws.data_ptr(),
@@ -313,9 +340,10 @@ def tsmttsm_split(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor | None = Non
         _check_operand(C, "C", torch.float64)
     lib = _capi.load()
     with torch.cuda.device(A.device):
-        sh = _stream_handle(A.device, stream)
+        so = _stream(A.device, stream)
+        sh = int(so.cuda_stream)
         need = lib.tsm_gemm_tn_workspace_size(n, m, k)
-        ws = workspace(A.device, need, sh)
+        ws = workspace(A.device, need, so)
         if kind == "tf32":
             st = lib.tsm_gemm_tn_f32_split(sh, n, m, k, A.data_ptr(), _ld(A), B.data_ptr(), _ld(B), C.data_ptr(),
                                            _ld(C), 1 if accumulate else 0, ws.data_ptr(), ws.numel())

@@ -14,7 +14,7 @@ import ctypes
 import torch
 
 from . import _capi
-from .api import _stream_handle
+from .api import _stream
 
 
 class BatchedTSMTTSM:
@@ -42,13 +42,17 @@ class BatchedTSMTTSM:
             nbytes = lib.tsm_batched_plan_size_f64(len(As), probs)
             if nbytes == 0:
                 raise _capi.TsmError(4, "batched plan: a problem is invalid or outside widths {4, 8, 16, 32}")
-            self.buffer = torch.zeros(nbytes, dtype=torch.uint8, device=dev)
+            so = _stream(dev, stream)
+            # allocated and zeroed on the stream the plan is written on (the
+            # init below copies on it and synchronises it)
+            with torch.cuda.stream(so):
+                self.buffer = torch.zeros(nbytes, dtype=torch.uint8, device=dev)
             self.plan = _capi.BatchedPlan()
-            sh = _stream_handle(dev, stream)
-            st = lib.tsm_batched_plan_init_f64(sh, len(As), probs, self.buffer.data_ptr(), nbytes,
+            st = lib.tsm_batched_plan_init_f64(int(so.cuda_stream), len(As), probs, self.buffer.data_ptr(), nbytes,
                                                ctypes.byref(self.plan))
             _capi.check(st, "tsm_batched_plan_init_f64")
         self.device = dev
+        self._alloc_stream = int(so.cuda_stream)
 
     @property
     def segments(self) -> int:
@@ -58,7 +62,13 @@ class BatchedTSMTTSM:
         """One launch computing every product; returns the list of C."""
         lib = _capi.load()
         with torch.cuda.device(self.device):
-            st = lib.tsm_gemm_tn_batched_f64(_stream_handle(self.device, stream), ctypes.byref(self.plan))
+            so = _stream(self.device, stream)
+            if int(so.cuda_stream) != self._alloc_stream and not torch.cuda.is_current_stream_capturing():
+                # the plan's counters are used on another stream: the caching
+                # allocator must not reuse the buffer before that work ends
+                # (a captured graph's replays are the caller's to order)
+                self.buffer.record_stream(so)
+            st = lib.tsm_gemm_tn_batched_f64(int(so.cuda_stream), ctypes.byref(self.plan))
         _capi.check(st, "tsm_gemm_tn_batched_f64")
         return self.Cs
 

@@ -488,7 +488,11 @@ tsm_status tsm_fill_uniform_f64(tsm_stream_t stream, double* x, int64_t count, u
 //     wrong results: serialise them.
 //   * The first call on each device looks the array's device address up
 //     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture.
+//     before any stream capture.  Like every per-device state of the
+//     library, that address does not survive cudaDeviceReset: do not reset a
+//     device while the library is in use on it.
+//   * A kernel that gives up a bounded wait sets a bit in the array's error
+//     word; tsm_noalloc_check reads and clears it.
 // ---------------------------------------------------------------------------
 namespace tsm {
 namespace {
@@ -566,4 +570,19 @@ extern "C" tsm_status tsm_gemm_tn_f64_noalloc(tsm_stream_t stream, int64_t n, in
   cudaError_t e = cudaMemsetAsync(p.counter, 0, sizeof(unsigned), cs);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(static scratch counter)");
   return launch_variant(v, p, grid, cs);
+}
+
+// Reads and clears the error word of the static scratch: the counterpart of
+// tsm_workspace_check for tsm_gemm_tn_f64_noalloc, whose kernels record a
+// bounded wait that ran out there instead of in a caller's workspace.  The
+// word is sticky across calls until read.  Allocates nothing.
+extern "C" tsm_status tsm_noalloc_check(tsm_stream_t stream, unsigned* bits) {
+  using namespace tsm;
+  int dev = 0;
+  DeviceState* st = nullptr;
+  tsm_status s = current_device(&dev, &st);
+  if (s != TSM_SUCCESS) return s;
+  void* scratch = nullptr;
+  if ((s = static_scratch(dev, &scratch)) != TSM_SUCCESS) return s;
+  return tsm_workspace_check(stream, scratch, bits);
 }
