@@ -83,6 +83,20 @@ tsm_status tsm_gemm_tn_f64_variant(tsm_stream_t stream, int64_t n, int m, int k,
                                    const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
                                    void* workspace, size_t workspace_bytes, int variant);
 
+/* Same as tsm_gemm_tn_f64_variant, launching at most max_ctas CTAs (<= 0:
+ * the variant's own grid, one or a few CTAs per SM; max_ctas never raises
+ * it).  Every kernel deals its rows over whatever grid it gets, so the
+ * result is the same product; the last CTA's sum over the per-CTA partials
+ * follows the grid, so bits may differ from another grid's.  Replaces the
+ * launch-size parameters of the reference: `stride` (the work-item count of
+ * tsmttsm.hh:15-439 and of the generated kernels, sycl_codegen.py:466,
+ * sycl_codegen_new.py:594) with `local_size` (:468, :596) -- a caller maps
+ * stride / local_size work-groups to CTAs, as the generated drop-in header
+ * does. */
+tsm_status tsm_gemm_tn_f64_launch(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                                  const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
+                                  void* workspace, size_t workspace_bytes, int variant, int64_t max_ctas);
+
 /* C = A^T B or C += A^T B with FP32 storage (A, B, C float).  Each thread
  * accumulates in FP32 over its rows; every sum across threads and CTAs is
  * FP64, then rounded once to FP32.  The FP32 forward of the autograd form
@@ -305,6 +319,19 @@ size_t tsm_batched_plan_size_f64(int count, const tsm_batched_problem_f64* probl
  * baked into the plan: re-initialise it when they change. */
 tsm_status tsm_batched_plan_init_f64(tsm_stream_t stream, int count, const tsm_batched_problem_f64* problems,
                                      void* device_buffer, size_t device_bytes, tsm_batched_plan* plan);
+
+/* The same, with the consumer path of each width class chosen by the
+ * caller: class_paths[4 log2(m / 4) + log2(k / 4)] is -1 (the autotuned
+ * choice, as tsm_batched_plan_init_f64 makes it), 0 (the class's default
+ * path: the FP64 tensor cores when m, k >= 16, SIMT register tiles below) or
+ * 1 (SIMT 4 x 4 register tiles over 1-D bulk copies; only the tensor-core
+ * classes have this second path, the others ignore it).  class_paths may be
+ * NULL (all -1).  The autotuner times both paths of each tensor-core class
+ * inside the batched launch through this call.  No counterpart in the
+ * reference. */
+tsm_status tsm_batched_plan_init_paths_f64(tsm_stream_t stream, int count, const tsm_batched_problem_f64* problems,
+                                           const int* class_paths, void* device_buffer, size_t device_bytes,
+                                           tsm_batched_plan* plan);
 
 /* Runs every product of the plan in ONE persistent launch (capturable in a
  * CUDA graph; the plan's first execution, or any other call, must happen

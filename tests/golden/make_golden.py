@@ -18,7 +18,10 @@ these are outputs of its own functions run on the host:
                          main.cc's launch shape (stride 16384, local size
                          32, tile 4), plus input samples;
   ref_variants.npz       all nine tsmttsm.hh variants and the kernels the
-                         two generators emit by default, M = 8, n = 4099.
+                         two generators emit by default, M = 8, n = 4099;
+  ref_codegen.json       the generators' command lines (sycl_codegen.py,
+                         sycl_codegen_new.py run as scripts) on a few flag
+                         sets: exit code, kernel names, stride.
 
 The inputs are not stored: tests regenerate them with the oracle's
 generators (pinned to the reference's by tests/test_oracle.py).
@@ -36,6 +39,8 @@ from __future__ import annotations
 import ctypes
 import json
 import os
+import re
+import subprocess
 import sys
 
 import numpy as np
@@ -50,6 +55,17 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 SQUARE_CASES = [  # (n, M, seed)
     (1, 1, 11), (2, 2, 12), (3, 4, 13), (17, 8, 14), (1000, 16, 15), (4099, 8, 16),
     (4097, 32, 17), (2049, 64, 18), (65536, 4, 19), (100003, 1, 20), (31, 64, 21), (8192, 16, 22),
+]
+
+# Command lines run through both reference generators (ref_codegen.json).
+CODEGEN_FLAG_SETS = [
+    [],
+    ["--with-benchmark"],
+    ["--M", "4", "8", "16", "32", "64", "--tile-sizes", "2", "4", "8", "--with-benchmark"],
+    ["--M", "12", "48", "--tile-sizes", "3", "4", "6"],
+    ["--M", "8", "--stride", "1000"],
+    ["--M", "12", "--stride", "4096"],
+    ["--M", "16", "--local-size", "128", "--unroll", "2"],
 ]
 
 MAIN_CC_SHAPE = dict(n=1 << 20, M=8, stride=16384, tile=4)
@@ -122,6 +138,24 @@ def main() -> int:
         var[name] = C.reshape(M, M)
     np.savez_compressed(os.path.join(OUT, "ref_variants.npz"), **var)
     meta["variants"] = VARIANTS_SHAPE
+
+    # 4. The generators' command lines (sycl_codegen.py, sycl_codegen_new.py
+    #    run as scripts): for each flag set, the exit code, the kernel names
+    #    in order, the stride the v2 script prints, and whether run_all_benchmarks
+    #    is emitted.
+    codegen = []
+    for style, script in (("v2", "sycl_codegen_new.py"), ("v1", "sycl_codegen.py")):
+        for flags in CODEGEN_FLAG_SETS:
+            r = subprocess.run([sys.executable, os.path.join(oracle.reference_dir(), script), *flags],
+                               capture_output=True, text=True)
+            names = re.findall(r"sycl::event (tsmttsm_[0-9a-z_]+)\(", r.stdout)
+            m = re.search(r"stride=(\d+)\s+local_size=(\d+)", r.stdout)
+            codegen.append({"style": style, "flags": flags, "rc": r.returncode, "names": names,
+                            "stride": int(m.group(1)) if m else None,
+                            "benchmark": "run_all_benchmarks" in r.stdout})
+    with open(os.path.join(OUT, "ref_codegen.json"), "w") as f:
+        json.dump(codegen, f, indent=0)
+        f.write("\n")
 
     with open(os.path.join(OUT, "golden_meta.json"), "w") as f:
         json.dump(meta, f, indent=1)

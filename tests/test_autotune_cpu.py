@@ -82,3 +82,19 @@ def test_committed_tuned_table_is_consistent():
     from tsm_benchmark_b200.autotune import SWEEP_PAIRS
     for m, k in SWEEP_PAIRS:
         assert (m, k, BUCKETS[-1][0]) in seen, (m, k)
+
+
+def test_batched_paths_reach_the_generated_table(tmp_path):
+    """tuned.json's batched_paths become the library's per-class table
+    (kTunedBatchedPaths in csrc/generated/variants_index.cu): 0 for the
+    tensor cores, 1 for SIMT register tiles."""
+    import json
+
+    from tsm_benchmark_b200 import codegen
+    doc = {"choices": [], "batched_paths": [{"m": 16, "k": 16, "path": "simt"}, {"m": 32, "k": 32, "path": "dmma"}]}
+    path = tmp_path / "tuned.json"
+    path.write_text(json.dumps(doc))
+    assert codegen.load_tuned_batched(str(path)) == [(16, 16, 1), (32, 32, 0)]
+    files = codegen.render(codegen.default_variants(), [], batched_paths=codegen.load_tuned_batched(str(path)))
+    idx = files["variants_index.cu"]
+    assert '"16 16 1",' in idx and '"32 32 0",' in idx and "kTunedBatchedPathCount = 2;" in idx

@@ -100,3 +100,40 @@ def test_batched_full_config_against_plain(gpu, oracle_mod):
         assert float(torch.linalg.norm(C - ref)) <= bound
     del As, Bs
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("path", ["dmma", "simt"])
+def test_batched_both_paths_of_the_tensor_core_classes(gpu, oracle_mod, path):
+    """The tensor-core classes (m, k in {16, 32}) have two compiled consumer
+    paths, FP64 tensor cores and SIMT register tiles; each, forced for every
+    class through the plan, matches the oracle on ragged problems mixed with
+    the SIMT-only classes (whose path the override leaves alone)."""
+    from tsm_benchmark_b200 import BatchedTSMTTSM
+    rng = np.random.default_rng(21)
+    shapes = [(int(n), m, k) for n, m, k in zip(rng.integers(1, 30000, size=40), rng.choice(WIDTHS, size=40),
+                                                 rng.choice(WIDTHS, size=40))]
+    shapes += [(70001, 16, 16), (65537, 16, 32), (33333, 32, 16), (100003, 32, 32), (3, 32, 32), (0, 16, 16)]
+    As, Bs, host = [], [], []
+    for i, (n, m, k) in enumerate(shapes):
+        A, B = oracle_mod.operands(n, m, k, 900 + i)
+        As.append(torch.from_numpy(A).to(gpu))
+        Bs.append(torch.from_numpy(B).to(gpu))
+        host.append((A, B))
+    paths = {(m, k): path for m in (16, 32) for k in (16, 32)}
+    Cs = BatchedTSMTTSM(As, Bs, class_paths=paths).run()
+    torch.cuda.synchronize()
+    for i, ((A, B), C) in enumerate(zip(host, Cs)):
+        ref = oracle_mod.naive(A, B)
+        got = C.cpu().numpy()
+        assert oracle_mod.check(ref, got) == -1, (path, shapes[i])
+        nw = oracle_mod.normwise(A, B, ref, got)
+        assert nw["err"] <= nw["bound"], (path, shapes[i], nw)
+
+
+def test_batched_class_paths_argument_errors(gpu):
+    from tsm_benchmark_b200 import BatchedTSMTTSM
+    A = torch.zeros((10, 16), dtype=torch.float64, device=gpu)
+    with pytest.raises(ValueError):
+        BatchedTSMTTSM([A], [A], class_paths={(16, 16): "tensor"})
+    with pytest.raises(ValueError):
+        BatchedTSMTTSM([A], [A], class_paths={(12, 16): "simt"})

@@ -140,3 +140,60 @@ def test_c_abi_rejects_bad_arguments_before_any_cuda_call():
     assert lib.tsm_selftest_wait_timeout(None, None, 0, 1000) == WORKSPACE
     assert lib.tsm_fill_uniform_f64(None, P, -1, 1, 0) == INVALID
     assert lib.tsm_fill_uniform_f64(None, P, 0, 1, 0) == 0
+
+
+def test_generator_command_line_matches_the_reference_generators():
+    """`python -m tsm_benchmark_b200.codegen` with the reference generators'
+    flags (--M, --tile-sizes, --stride, --local-size, --unroll,
+    --with-benchmark; --style v1 for sycl_codegen.py's names) against the
+    reference scripts' own output on the same flag sets
+    (tests/golden/ref_codegen.json): same exit status, same kernel names in
+    the same order, the same automatic stride, run_all_benchmarks exactly
+    when asked for."""
+    import contextlib
+    import io
+    import json
+    import re
+
+    from tests.conftest import GOLDEN
+    from tsm_benchmark_b200 import codegen
+    with open(os.path.join(GOLDEN, "ref_codegen.json")) as f:
+        cases = json.load(f)
+    assert len(cases) >= 14
+    for case in cases:
+        out, err = io.StringIO(), io.StringIO()
+        with contextlib.redirect_stdout(out), contextlib.redirect_stderr(err):
+            rc = codegen.main(["--style", case["style"], *case["flags"]])
+        what = (case["style"], case["flags"])
+        assert (rc != 0) == (case["rc"] != 0), (what, err.getvalue())
+        if rc:
+            assert err.getvalue().strip(), what
+            continue
+        text = out.getvalue()
+        assert re.findall(r"sycl::event (tsmttsm_[0-9a-z_]+)\(", text) == case["names"], what
+        if case["stride"] is not None:
+            assert re.search(r"stride=(\d+)\s+local_size", text).group(1) == str(case["stride"]), what
+        assert ("run_all_benchmarks" in text) == case["benchmark"], what
+
+
+def test_generated_kernels_name_compiled_variants():
+    """Every kernel of a generated header runs a variant the library has, and
+    the four names of a (M, TM) pair run distinct kernels wherever the
+    library compiles distinct ring depths for that tile."""
+    import re
+
+    from tsm_benchmark_b200 import codegen
+    vs = codegen.default_variants()
+    names = {v.name for v in vs}
+    text = codegen.render_dropin_header(vs, widths=(4, 8, 16, 32, 64), tiles=(2, 4, 8))
+    picked = re.findall(r'variant_by_name\("([^"]+)"\)', text)
+    assert picked and set(picked) <= names
+    # 8 x 8 with 4 x 4 tiles: deepest ring, double buffer, tuned default, middle ring
+    kinds = [codegen.pick_dropin_variant(vs, 8, 4, lf, sg)[0] for lf, sg in
+             ((False, False), (True, False), (False, True), (True, True))]
+    assert kinds[2] is None and len({kinds[0], kinds[1], kinds[3]}) == 3
+    # widths 16..64: the prefetching reduction-optimised name runs the FP64 tensor cores
+    for m in (16, 32, 64):
+        assert codegen.pick_dropin_variant(vs, m, 4, True, True)[0].startswith("dmma_")
+    # the CTA cap is stride / local_size work-groups
+    assert "K, 8, 8, A, B, C, variant, 2048);" in codegen.render_dropin_header(vs, widths=(8,), tiles=(4,))

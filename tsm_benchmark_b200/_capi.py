@@ -80,6 +80,8 @@ SIGNATURES = {
                                         c_int64, c_int64, c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_f64_variant": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int, c_void_p, c_size_t, c_int]),
+    "tsm_gemm_tn_f64_launch": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
+                                       c_void_p, c_int64, c_int, c_void_p, c_size_t, c_int, c_int64]),
     "tsm_gemm_tn_f32": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                 c_void_p, c_int64, c_int, c_void_p, c_size_t]),
     "tsm_gemm_tn_f32_variant": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
@@ -109,6 +111,9 @@ SIGNATURES = {
     "tsm_batched_plan_size_f64": (c_size_t, [c_int, ctypes.POINTER(BatchedProblem)]),
     "tsm_batched_plan_init_f64": (c_int, [c_void_p, c_int, ctypes.POINTER(BatchedProblem), c_void_p, c_size_t,
                                           ctypes.POINTER(BatchedPlan)]),
+    "tsm_batched_plan_init_paths_f64": (c_int, [c_void_p, c_int, ctypes.POINTER(BatchedProblem),
+                                                ctypes.POINTER(c_int), c_void_p, c_size_t,
+                                                ctypes.POINTER(BatchedPlan)]),
     "tsm_gemm_tn_batched_f64": (c_int, [c_void_p, ctypes.POINTER(BatchedPlan)]),
     "tsm_gemm_tn_f64_noalloc": (c_int, [c_void_p, c_int64, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64,
                                         c_void_p, c_int64, c_int]),

@@ -2,6 +2,7 @@
 """Autotuner: picks the fastest compiled variant per (m, k, n-bucket, dtype).
 
     python -m tsm_benchmark_b200.autotune [--shapes sweep|batched|all] [--out tuned.json]
+    python -m tsm_benchmark_b200.autotune --shapes batched-paths   (the batched kernel's path per class)
     python -m tsm_benchmark_b200.autotune --pairs 8x8 --merge        (re-tune one shape, keep the rest)
 
 For every width pair and row bucket it times each applicable variant of the
@@ -173,15 +174,81 @@ def tune(pairs, buckets=BUCKETS, reps_time_ms: float = 150.0, verbose: bool = Tr
             "choices": choices, "timings": timings}
 
 
+# Width classes of the batched kernel with two compiled consumer paths.
+BATCHED_TC_CLASSES = [(16, 16), (16, 32), (32, 16), (32, 32)]
+
+
+def tune_batched_paths(count: int = 96, rounds: int = 5, reps: int = 10, seed: int = 11,
+                       verbose: bool = True) -> list[dict]:
+    """For each tensor-core class of the batched kernel, both consumer paths
+    (FP64 tensor cores, SIMT register tiles) timed inside the batched launch
+    on `count` problems of that class (n log-uniform in [10^4, 10^6], the
+    upper part of the batched configuration's range), in interleaved rounds;
+    the path with the smaller median wins.  Both paths' results must agree
+    within the normwise bound first."""
+    import numpy as np
+    import torch
+
+    from .api import fill_uniform
+    from .batched import BatchedTSMTTSM
+
+    dev = torch.device("cuda", 0)
+    out = []
+    for m, k in BATCHED_TC_CLASSES:
+        rng = np.random.default_rng(seed + m + 3 * k)
+        ns = np.exp(rng.uniform(np.log(1e4), np.log(1e6), size=count)).astype(np.int64)
+        As, Bs = [], []
+        for i, n in enumerate(ns):
+            a = torch.empty((int(n), m), dtype=torch.float64, device=dev)
+            b = torch.empty((int(n), k), dtype=torch.float64, device=dev)
+            fill_uniform(a, 100 + i, 0)
+            fill_uniform(b, 100 + i, 1)
+            As.append(a)
+            Bs.append(b)
+        plans = {path: BatchedTSMTTSM(As, Bs, class_paths={(m, k): path}) for path in ("dmma", "simt")}
+        res = {path: [c.clone() for c in p.run()] for path, p in plans.items()}
+        for a, b, c0, c1 in zip(As, Bs, res["dmma"], res["simt"]):
+            bound = 8 * math.sqrt(a.shape[0]) * 2.0**-53 * float(torch.linalg.norm(a)) * float(torch.linalg.norm(b))
+            if float(torch.linalg.norm(c0 - c1)) > bound:
+                raise RuntimeError(f"batched paths disagree for class {m}x{k}")
+        samples = {path: [] for path in plans}
+        for _ in range(rounds):
+            for path, p in plans.items():
+                samples[path].append(time_variant(p.run, reps, warmup=1))
+        win, med = median_winner(samples)
+        nbytes = int(sum(8 * int(n) * (m + k) for n in ns))
+        out.append({"m": m, "k": k, "path": win, "problems": count, "bytes": nbytes,
+                    "median_ms": {path: round(t, 5) for path, t in med.items()}})
+        if verbose:
+            print(f"batched {m:>2}x{k:<2}: {win:<5} " + ", ".join(
+                f"{path} {t:.4f} ms ({nbytes / (t * 1e-3) / 1e9:.0f} GB/s)" for path, t in med.items()), flush=True)
+        del As, Bs, plans, res
+        torch.cuda.empty_cache()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--shapes", choices=["sweep", "batched", "all"], default="all")
+    ap.add_argument("--shapes", choices=["sweep", "batched", "batched-paths", "all"], default="all",
+                    help="batched-paths: the batched kernel's consumer path per tensor-core class "
+                         "(kept beside the other choices of --out)")
     ap.add_argument("--out", default=DEFAULT_OUT)
     ap.add_argument("--budget-ms", type=float, default=150.0, help="timed milliseconds per candidate")
     ap.add_argument("--pairs", default=None, help="only these width pairs, e.g. 8x8,16x16 (overrides --shapes)")
     ap.add_argument("--merge", action="store_true",
                     help="keep the other pairs' choices and timings of an existing --out file")
     args = ap.parse_args(argv)
+    if args.shapes == "batched-paths":
+        old = {}
+        if os.path.exists(args.out):
+            with open(args.out) as f:
+                old = json.load(f)
+        old["batched_paths"] = tune_batched_paths()
+        with open(args.out, "w") as f:
+            json.dump(old, f, indent=1)
+            f.write("\n")
+        print(f"wrote {args.out}: {len(old['batched_paths'])} batched paths")
+        return 0
     pairs = {"sweep": SWEEP_PAIRS, "batched": BATCHED_PAIRS,
              "all": sorted(set(SWEEP_PAIRS + BATCHED_PAIRS))}[args.shapes]
     if args.pairs:
@@ -190,6 +257,11 @@ def main(argv=None) -> int:
     if args.merge and os.path.exists(args.out):
         with open(args.out) as f:
             res = merge_results(json.load(f), res, pairs)
+    if os.path.exists(args.out) and "batched_paths" not in res:
+        with open(args.out) as f:
+            kept = json.load(f).get("batched_paths")
+        if kept:
+            res["batched_paths"] = kept
     with open(args.out, "w") as f:
         json.dump(res, f, indent=1)
         f.write("\n")

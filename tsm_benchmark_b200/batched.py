@@ -17,10 +17,25 @@ from . import _capi
 from .api import _stream
 
 
+_PATHS = {"dmma": 0, "simt": 1}
+_WIDTHS = (4, 8, 16, 32)
+
+
+def _class_index(m: int, k: int) -> int:
+    """Width class of the batched kernel: 4 log2(m / 4) + log2(k / 4)."""
+    if m not in _WIDTHS or k not in _WIDTHS:
+        return -1
+    return 4 * _WIDTHS.index(m) + _WIDTHS.index(k)
+
+
 class BatchedTSMTTSM:
     """A plan for C_p = A_p^T B_p (p = 0 .. count-1) and its launch."""
 
-    def __init__(self, As, Bs, Cs=None, *, accumulate: bool = False, stream: torch.cuda.Stream | None = None):
+    def __init__(self, As, Bs, Cs=None, *, accumulate: bool = False, stream: torch.cuda.Stream | None = None,
+                 class_paths: dict | None = None):
+        """``class_paths`` maps a width class (m, k) to its consumer path,
+        "dmma" (the FP64 tensor cores, the default of m, k >= 16) or "simt"
+        (SIMT register tiles); classes not named take the autotuned path."""
         if len(As) != len(Bs) or not As:
             raise ValueError("As and Bs must be non-empty and of equal length")
         dev = As[0].device
@@ -48,9 +63,17 @@ class BatchedTSMTTSM:
             with torch.cuda.stream(so):
                 self.buffer = torch.zeros(nbytes, dtype=torch.uint8, device=dev)
             self.plan = _capi.BatchedPlan()
-            st = lib.tsm_batched_plan_init_f64(int(so.cuda_stream), len(As), probs, self.buffer.data_ptr(), nbytes,
-                                               ctypes.byref(self.plan))
-            _capi.check(st, "tsm_batched_plan_init_f64")
+            paths = None
+            if class_paths:
+                paths = (ctypes.c_int * 16)(*([-1] * 16))
+                for (m, k), name in class_paths.items():
+                    cls = _class_index(m, k)
+                    if cls < 0 or name not in _PATHS:
+                        raise ValueError(f"class_paths: ({m}, {k}) -> {name!r}")
+                    paths[cls] = _PATHS[name]
+            st = lib.tsm_batched_plan_init_paths_f64(int(so.cuda_stream), len(As), probs, paths,
+                                                     self.buffer.data_ptr(), nbytes, ctypes.byref(self.plan))
+            _capi.check(st, "tsm_batched_plan_init_paths_f64")
         self.device = dev
         self._alloc_stream = int(so.cuda_stream)
 

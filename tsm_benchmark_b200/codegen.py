@@ -33,6 +33,11 @@ Usage::
     python -m tsm_benchmark_b200.codegen --check    # exit 1 if out of date
     python -m tsm_benchmark_b200.codegen --list     # print the variant names
 
+    # the reference generators' command line: the drop-in header on stdout
+    python -m tsm_benchmark_b200.codegen --M 4 8 16 32 --tile-sizes 2 4 \\
+        [--stride S] [--local-size L] [--sg-size 32] [--unroll U] \\
+        [--with-benchmark] [--style v1|v2] > tsmttsm_kernels.hh
+
 The emitted files are committed; tests check that regenerating reproduces
 them byte for byte.
 """
@@ -415,6 +420,20 @@ def check_variants(vs: Iterable) -> None:
         names.add(v.name)
 
 
+BATCHED_PATHS = {"dmma": 0, "simt": 1}
+
+
+def load_tuned_batched(path: str = TUNED_JSON) -> list[tuple[int, int, int]]:
+    """Tuned consumer path per width class of the batched kernel: list of
+    (m, k, path), path 0 = the class's default (FP64 tensor cores for m, k
+    >= 16), 1 = SIMT register tiles."""
+    if not os.path.exists(path):
+        return []
+    with open(path) as f:
+        doc = json.load(f)
+    return sorted((int(e["m"]), int(e["k"]), BATCHED_PATHS[e["path"]]) for e in doc.get("batched_paths", []))
+
+
 def load_tuned(path: str = TUNED_JSON) -> list[tuple[int, int, int, str]]:
     """Tuned defaults: list of (m, k, nmin, variant name)."""
     if not os.path.exists(path):
@@ -431,8 +450,10 @@ HEADER = ("// Generated by tsm_benchmark_b200/codegen.py -- do not edit.\n"
           "// Regenerate with: python -m tsm_benchmark_b200.codegen\n")
 
 
-def render(vs: list, tuned: list, parts: int = 8) -> dict[str, str]:
+def render(vs: list, tuned: list, parts: int = 8, batched_paths: list | None = None) -> dict[str, str]:
     """Returns {file name: contents} for csrc/generated/."""
+    if batched_paths is None:
+        batched_paths = load_tuned_batched()
     check_variants(vs)
     known = {v.name for v in vs}
     for m, k, nmin, name in tuned:
@@ -475,77 +496,236 @@ def render(vs: list, tuned: list, parts: int = 8) -> dict[str, str]:
     idx.append("extern const int kTunedDefaultCount;")
     idx.append(f"const int kTunedDefaultCount = {len(tuned)};")
     idx.append("")
+    idx.append("// Tuned consumer paths of the batched kernel: \"m k path\" (0 tensor cores, 1 SIMT).")
+    idx.append("extern const char* const kTunedBatchedPaths[];")
+    idx.append("const char* const kTunedBatchedPaths[] = {")
+    for m, k, path in batched_paths:
+        idx.append(f'    "{m} {k} {path}",')
+    idx.append("    nullptr};")
+    idx.append("extern const int kTunedBatchedPathCount;")
+    idx.append(f"const int kTunedBatchedPathCount = {len(batched_paths)};")
+    idx.append("")
     idx.append("}  // namespace tsm")
     files["variants_index.cu"] = "\n".join(idx) + "\n"
     return files
 
 
 COMPAT_HEADER = os.path.join(HERE, "compat", "tsmttsm_kernels.hh")
-COMPAT_SUFFIXES = ("", "_lf", "_sg", "_sg_lf")
+
+# The four kernel names the reference generators emit per (M, TM), as
+# (prefetch, reduction-optimised) options, with the benchmark labels their
+# harnesses print: v2 sycl_codegen_new.py:153,257 (basic, _lf, _sg, _sg_lf);
+# v1 sycl_codegen.py:38-44 (_tr, _lf_tr, _2l_tr, _lf_2l_tr).
+DROPIN_STYLES = {
+    "v2": [("", False, False, "basic"), ("_lf", True, False, "lf"), ("_sg", False, True, "sg"),
+           ("_sg_lf", True, True, "sg_lf")],
+    "v1": [("_tr", False, False, "basic"), ("_lf_tr", True, False, "leapfrog"), ("_2l_tr", False, True, "2level"),
+           ("_lf_2l_tr", True, True, "all")],
+}
 
 
-def compat_variant_for(vs: list, m: int, tm: int) -> str | None:
-    """The exact bulk variant whose register tile is the reference's TM x TM
-    for width m, else None (the library default is used)."""
-    for v in vs:
-        if isinstance(v, BulkVariant) and v.exact and v.dtype == "f64" and not v.gram \
-                and (v.wa, v.wb, v.ta, v.tb) == (m, m, tm, tm) and v.unroll == 1 and v.cw == 8 and v.stages == 6:
-            return v.name
-    return None
+def dropin_name(style: str, m: int, tm: int, suffix: str) -> str:
+    base = f"tsmttsm_gen_{m}_{m}_{tm}_{tm}" if style == "v1" else f"tsmttsm_{m}_{m}_{tm}_{tm}"
+    return base + suffix
 
 
-def render_compat_header(vs: list, widths=(4, 8, 16), tiles=(2, 4)) -> str:
-    """tsmttsm_kernels.hh for main_codegen.cc: the names sycl_codegen_new.py
-    emits (tsmttsm_{M}_{N}_{TM}_{TN}{,_lf,_sg,_sg_lf}, :153,:257) with its
-    signature (q, int K, const T* A, const T* B, T* C) (:159,:264), each a
-    library call pinned to the variant with the same register tile, and
-    run_all_benchmarks<T>(q, K, warmup, runs) (:417-419)."""
+def _covers(v, m: int) -> bool:
+    return (v.wa, v.wb) == (m, m) if v.exact else (v.wa >= m and v.wb >= m)
+
+
+def pick_dropin_variant(vs: list, m: int, tm: int, prefetch: bool, reduce_opt: bool, local_size: int = 256,
+                        unroll: int = 1) -> tuple[str | None, str]:
+    """The compiled FP64 variant a generated drop-in kernel runs, and why.
+
+    The reference's options map onto this library's axes as follows:
+      * TM -> the SIMT register tile TM x TM (the nearest compiled tile);
+      * leap-frog prefetch (_lf) -> the shared-memory ring: without it the
+        deepest compiled ring (many short bulk copies in flight), with it the
+        shallowest (a double buffer of long copies, the leap-frog's analogue);
+      * the reduction-optimised kernels (_sg / _2l) -> the autotuned choice
+        for (M, M, K) (FP64 tensor cores for widths 16..64), and with _lf the
+        tensor-core kernel's shallowest ring, or the SIMT tile's middle ring
+        below width 16;
+      * local_size -> consumer warps (local_size / 32) and --unroll -> the
+        row-loop unroll, where such a variant is compiled.
+    None means the library's autotuned default at run time."""
+    if reduce_opt and not prefetch:
+        return None, "chosen per (M, M, K) at run time; every kernel reduces with the two-level sum"
+    simt = [v for v in vs if isinstance(v, BulkVariant) and v.dtype == "f64" and not v.gram and _covers(v, m)
+            and v.ta == v.tb]
+    if reduce_opt and prefetch:
+        dm = [v.resolved() for v in vs if isinstance(v, DmmaVariant) and not v.gram and (v.wa, v.wb) == (m, m)]
+        if dm:
+            v = min(dm, key=lambda d: (d.stages, -d.rows))
+            return v.name if isinstance(v, DmmaVariant) else None, "FP64 tensor cores, shallowest ring"
+    if not simt:
+        return None, "no SIMT tile compiled for this width: the autotuned default"
+    exact = [v for v in simt if v.exact]
+    if exact:
+        pool = exact
+    else:  # the smallest capacity that covers the width
+        cap = min(v.wa for v in simt)
+        pool = [v for v in simt if v.wa == cap and v.wb == cap]
+
+    def tile_gap(v):
+        return abs(math.log2(v.ta) - math.log2(tm))
+
+    best_gap = min(tile_gap(v) for v in pool)
+    pool = [v for v in pool if tile_gap(v) == best_gap]
+    notes = []
+    if best_gap:
+        notes.append(f"no {tm}x{tm} tile compiled for width {m}: nearest tile {pool[0].ta}x{pool[0].ta}")
+    for axis, want, label in (("cw", local_size // 32, "local_size"), ("unroll", unroll, "unroll")):
+        hit = [v for v in pool if getattr(v, axis) == want]
+        if hit:
+            pool = hit
+        elif (axis == "cw" and want != 8) or (axis == "unroll" and want != 1):
+            notes.append(f"{label} {want * 32 if axis == 'cw' else want} not compiled for this tile")
+    if reduce_opt and prefetch:  # below width 16: the middle ring of the SIMT tile
+        depths = sorted({v.resolved().stages for v in pool})
+        want = depths[len(depths) // 2]
+        v = [u for u in pool if u.resolved().stages == want][0]
+        notes.insert(0, "SIMT tile, middle ring depth")
+    else:
+        key = (lambda u: (u.resolved().stages, -u.resolved().rows))
+        v = min(pool, key=key) if prefetch else max(pool, key=key)
+        notes.insert(0, "shallowest ring (double buffer)" if prefetch else "deepest ring")
+    return v.name, "; ".join(notes)
+
+
+def suggest_stride(widths, tiles, local_size: int, sg_size: int, target_groups: int = 2048) -> int:
+    """The work-item count the v2 generator picks when --stride is omitted
+    (sycl_codegen_new.py:561-580): the least common multiple of local_size
+    and, per (M, TM), the tile count and sg_size x tile count, scaled to
+    about `target_groups` work-groups."""
+    req = local_size
+    for m in widths:
+        for tm in tiles:
+            if m % tm:
+                continue
+            nt = (m // tm) ** 2
+            req = math.lcm(req, nt, sg_size * nt)
+    req = math.lcm(req, local_size)
+    return max(1, -(-local_size * target_groups // req)) * req
+
+
+def validate_launch(style: str, widths, tiles, stride: int, local_size: int, sg_size: int) -> list[str]:
+    """The reference generators' launch checks (sycl_codegen.py:475-491,
+    sycl_codegen_new.py:530-558, :609-611): returns the error lines; v1
+    only warns about uneven tile distribution (printed, not returned)."""
+    errs = []
+    if sg_size != 32:
+        errs.append(f"Error: --sg-size {sg_size}: the sub-group on B200 is the 32-thread warp")
+    if local_size % 32:
+        errs.append(f"Error: --local-size ({local_size}) must be a multiple of --sg-size (32)")
+    if stride % local_size:
+        errs.append(f"Error: --stride {stride} must be divisible by --local-size {local_size}")
+        return errs
+    for m in widths:
+        if not 1 <= m <= 64:
+            errs.append(f"Error: --M {m}: widths are 1..64")
+            continue
+        for tm in tiles:
+            if m % tm:
+                continue
+            nt = (m // tm) ** 2
+            if style == "v1":
+                if stride % (nt * local_size):
+                    print(f"Warning: --stride ({stride}) is not a multiple of num_tiles*local_size="
+                          f"{nt * local_size} for M={m}, TM={tm}.", file=sys.stderr)
+                continue
+            if stride % nt:
+                errs.append(f"Warning: stride ({stride}) not divisible by num_tiles ({nt}) for M={m}, TM={tm}"
+                            "  [basic/lf kernels]")
+            if (stride // sg_size) % nt:
+                errs.append(f"Warning: stride/sg_size ({stride // sg_size}) not divisible by num_tiles ({nt}) "
+                            f"for M={m}, TM={tm}  [sg kernels]")
+    return errs
+
+
+def render_dropin_header(vs: list, widths=(4, 8, 16), tiles=(2, 4), style: str = "v2", stride: int | None = None,
+                         local_size: int | None = None, sg_size: int = 32, unroll: int = 1,
+                         with_benchmark: bool = True) -> str:
+    """The header the reference generators print, for this library:
+    `sycl_codegen_new.py` (style v2: tsmttsm_{M}_{N}_{TM}_{TN}{,_lf,_sg,_sg_lf}
+    (q, int K, const T* A, const T* B, T* C), :153-159,257-264) or
+    `sycl_codegen.py` (style v1: tsmttsm_gen_{M}_{N}_{TM}_{TN}[_lf][_2l]_tr
+    (q, int K, T* A, T* B, T* C), :38-63), plus run_all_benchmarks<T>(q, K,
+    warmup, runs) (v2 :417-419, defaults 1 << 20, 10, 30; v1 :319, defaults
+    1024 * 1024, 50, 100) with --with-benchmark.  Each kernel adds A^T B into
+    C through tsm_gemm_tn_f64_launch: the variant pick_dropin_variant chose,
+    on at most stride / local_size CTAs (the reference's work-groups)."""
+    if local_size is None:
+        local_size = 32 if style == "v1" else 256
+    if stride is None:
+        stride = 16384 if style == "v1" else suggest_stride(widths, tiles, local_size, sg_size)
+    groups = stride // local_size
+    const = "const " if style == "v2" else ""
+    gen = "sycl_codegen.py" if style == "v1" else "sycl_codegen_new.py"
     out = [HEADER.rstrip("\n"), "//",
-           "// Drop-in for the header `sycl_codegen_new.py --with-benchmark` emits.",
-           "// Kernel names and signatures are the reference generator's; every kernel",
-           "// adds A^T B into C through tsm_gemm_tn_f64_variant on the queue's stream.",
-           "// The _lf / _sg / _sg_lf spellings name the reference's prefetch and",
-           "// sub-group-reduction options; every variant here prefetches through a",
-           "// multi-stage TMA ring and reduces with warp shuffles, so they share one",
-           "// variant per (M, TM).",
+           f"// Drop-in for the header `{gen}` emits, on libtsm_b200.so.",
+           "// Kernel names and signatures are the reference generator's; every kernel adds",
+           "// A^T B into C through tsm_gemm_tn_f64_launch on the queue's stream, with a",
+           "// compiled variant of this library (named above each kernel) on at most",
+           "// stride / local_size CTAs.",
+           f"//   widths {' '.join(map(str, widths))}; tiles {' '.join(map(str, tiles))}; stride={stride} "
+           f"local_size={local_size} sg_size={sg_size} unroll={unroll}",
            "#pragma once", "", "#include <sycl/sycl.hpp>", "", "#include <vector>", "",
            '#include "tsm_compat_bench.hh"', '#include "tsmttsm.hh"', ""]
     for m in widths:
+        out.append(f"// {'=' * 60}")
+        out.append(f"// M = {m}")
+        out.append(f"// {'=' * 60}")
+        out.append("")
         for tm in tiles:
             if m % tm:
                 continue
-            vname = compat_variant_for(vs, m, tm)
-            for suffix in COMPAT_SUFFIXES:
-                fname = f"tsmttsm_{m}_{m}_{tm}_{tm}{suffix}"
+            picked = {}
+            for suffix, prefetch, reduce_opt, _label in DROPIN_STYLES[style]:
+                vname, why = pick_dropin_variant(vs, m, tm, prefetch, reduce_opt, local_size, unroll)
+                fname = dropin_name(style, m, tm, suffix)
+                if vname is not None and vname in picked:
+                    why += f" (the same kernel as {picked[vname]}: no other ring compiled for this tile)"
+                picked.setdefault(vname, fname)
+                out.append(f"// runs {vname or 'the autotuned default'}: {why}")
                 out.append("template <typename T>")
-                out.append(f"sycl::event {fname}(sycl::queue& q, int K, const T* A, const T* B, T* C) {{")
+                out.append(f"sycl::event {fname}(sycl::queue& q, int K, {const}T* A, {const}T* B, T* C) {{")
                 if vname:
                     out.append(f'  static const int variant = tsm_compat::variant_by_name("{vname}");')
                 else:
-                    out.append("  static const int variant = -1;  // no variant with this tile: library default")
-                out.append(f"  return tsm_compat::accumulate_tn<T>(q, K, {m}, {m}, A, B, C, variant);")
+                    out.append("  static const int variant = -1;")
+                out.append(f"  return tsm_compat::accumulate_tn<T>(q, K, {m}, {m}, A, B, C, variant, {groups});")
                 out.append("}")
                 out.append("")
-    out.append("template <typename T>")
-    out.append("void run_all_benchmarks(sycl::queue& q, int K = 1 << 20, int warmup = 10, int runs = 30) {")
-    out.append('  std::cout << "Device: " << q.get_device().get_info<sycl::info::device::name>() << "\\n\\n";')
-    out.append("  std::vector<tsm_compat::BenchResult> results;")
-    for m in widths:
-        out.append("  {")
-        out.append(f"    tsm_compat::Problem<T> p(q, K, {m});")
-        for tm in tiles:
-            if m % tm:
-                continue
-            for suffix, label in zip(COMPAT_SUFFIXES, ("basic", "lf", "sg", "sg_lf")):
-                fname = f"tsmttsm_{m}_{m}_{tm}_{tm}{suffix}"
-                out.append(f'    results.push_back(p.bench("M{m}_T{tm}_{label}", '
-                           f"[&](int k) {{ return {fname}<T>(q, k, p.A, p.B, p.C); }}, warmup, runs));")
-        out.append("  }")
-    out.append("  tsm_compat::print_results(results);")
-    out.append("}")
-    out.append("")
+    if with_benchmark:
+        k_default, warm, runs, rel = ("1024 * 1024", 50, 100, "1e-8") if style == "v1" else ("1 << 20", 10, 30, "1e-6")
+        out.append("template <typename T>")
+        out.append(f"void run_all_benchmarks(sycl::queue& q, int K = {k_default}, int warmup = {warm}, "
+                   f"int runs = {runs}) {{")
+        out.append('  std::cout << "Device: " << q.get_device().get_info<sycl::info::device::name>() << "\\n\\n";')
+        out.append("  std::vector<tsm_compat::BenchResult> results;")
+        for m in widths:
+            out.append("  {")
+            out.append(f"    tsm_compat::Problem<T> p(q, K, {m}, 123, {rel});")
+            for tm in tiles:
+                if m % tm:
+                    continue
+                for suffix, _p, _r, label in DROPIN_STYLES[style]:
+                    fname = dropin_name(style, m, tm, suffix)
+                    out.append(f'    results.push_back(p.bench("M{m}_T{tm}_{label}", '
+                               f"[&](int k) {{ return {fname}<T>(q, k, p.A, p.B, p.C); }}, warmup, runs));")
+            out.append("  }")
+        out.append("  tsm_compat::print_results(results);")
+        out.append("}")
+        out.append("")
     out.append("// End of generated code")
     return "\n".join(out) + "\n"
+
+
+def render_compat_header(vs: list) -> str:
+    """compat/tsmttsm_kernels.hh: the v2 header with the reference
+    generator's defaults (--M 4 8 16 --tile-sizes 2 4 --with-benchmark)."""
+    return render_dropin_header(vs)
 
 
 def write(files: dict[str, str], out_dir: str = GEN_DIR) -> None:
@@ -569,7 +749,14 @@ def is_current(files: dict[str, str], out_dir: str = GEN_DIR) -> bool:
     return True
 
 
+REFERENCE_FLAGS = ("--M", "--tile-sizes", "--stride", "--local-size", "--sg-size", "--unroll", "--with-benchmark",
+                   "--style")
+
+
 def main(argv=None) -> int:
+    argv = sys.argv[1:] if argv is None else list(argv)
+    if any(a.split("=")[0] in REFERENCE_FLAGS for a in argv):
+        return main_dropin(argv)
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--check", action="store_true", help="exit 1 if csrc/generated is stale")
     ap.add_argument("--list", action="store_true", help="print the variant names")
@@ -591,6 +778,38 @@ def main(argv=None) -> int:
         with open(COMPAT_HEADER, "w") as f:
             f.write(compat)
     print(f"wrote {len(files)} files, {len(vs)} variants, {len(load_tuned())} tuned choices to {args.out}")
+    return 0
+
+
+def main_dropin(argv) -> int:
+    """The reference generators' command line: prints the drop-in header on
+    stdout, e.g. ``python -m tsm_benchmark_b200.codegen --M 4 8 16 32
+    --tile-sizes 2 4 --with-benchmark > tsmttsm_kernels.hh`` (v2 names) or
+    the same with ``--style v1``.  Flags and defaults as in
+    sycl_codegen_new.py:587-603 (v2) and sycl_codegen.py:461-473 (v1)."""
+    ap = argparse.ArgumentParser(description="Generate the drop-in tsmttsm_kernels.hh for libtsm_b200.so")
+    ap.add_argument("--style", choices=("v1", "v2"), default="v2",
+                    help="v2: sycl_codegen_new.py names (default); v1: sycl_codegen.py names")
+    ap.add_argument("--M", type=int, nargs="+", default=[4, 8, 16], help="Matrix sizes (default: 4 8 16)")
+    ap.add_argument("--tile-sizes", type=int, nargs="+", default=[2, 4], help="Tile sizes TM=TN (default: 2 4)")
+    ap.add_argument("--stride", type=int, default=None,
+                    help="Total work-item count (v1 default 16384; v2: auto-computed if omitted)")
+    ap.add_argument("--local-size", type=int, default=None, help="Work-group size (v1 default 32, v2 256)")
+    ap.add_argument("--sg-size", type=int, default=32, help="Sub-group size: the warp, 32")
+    ap.add_argument("--unroll", type=int, default=1, help="Row-loop unroll factor (default: 1)")
+    ap.add_argument("--with-benchmark", action="store_true", help="Append run_all_benchmarks<T>")
+    args = ap.parse_args(argv)
+    local = args.local_size if args.local_size is not None else (32 if args.style == "v1" else 256)
+    stride = args.stride
+    if stride is None:
+        stride = 16384 if args.style == "v1" else suggest_stride(args.M, args.tile_sizes, local, args.sg_size)
+    errs = validate_launch(args.style, args.M, args.tile_sizes, stride, local, args.sg_size)
+    if errs:
+        for e in errs:
+            print(e, file=sys.stderr)
+        return 1
+    sys.stdout.write(render_dropin_header(default_variants(), args.M, args.tile_sizes, args.style, stride, local,
+                                          args.sg_size, args.unroll, args.with_benchmark))
     return 0
 
 

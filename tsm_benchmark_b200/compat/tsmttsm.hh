@@ -30,16 +30,18 @@
 
 namespace tsm_compat {
 
+// C += A^T B on the queue's stream with the given variant (-1: the tuned
+// default) on at most max_ctas CTAs (0: the variant's own grid).
 template <class T>
 sycl::event accumulate_tn(sycl::queue& q, long long K, int M, int N, const T* A, const T* B, T* C,
-                          int variant = -1) {
+                          int variant = -1, long long max_ctas = 0) {
   static_assert(std::is_same_v<T, double>, "the plain path is FP64 (T = double)");
   const size_t ws_bytes = tsm_gemm_tn_workspace_size(K, M, N);
   if (ws_bytes == 0) throw sycl::exception("tsmttsm: unsupported width or no CUDA device");
   void* ws = q.workspace(ws_bytes);
   sycl::event e = q.begin();
-  const tsm_status st = tsm_gemm_tn_f64_variant(q.native_stream(), K, M, N, A, M, B, N, C, N, /*accumulate=*/1, ws,
-                                                q.workspace_bytes(), variant);
+  const tsm_status st = tsm_gemm_tn_f64_launch(q.native_stream(), K, M, N, A, M, B, N, C, N, /*accumulate=*/1, ws,
+                                               q.workspace_bytes(), variant, max_ctas);
   if (st != TSM_SUCCESS)
     throw sycl::exception(std::string("tsm_gemm_tn_f64: ") + tsm_status_string(st) + " " + tsm_last_cuda_error());
   e.record_end();

@@ -66,10 +66,40 @@ tsm_status fail(cudaError_t e, const char* what) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+}  // namespace
+
+// Autotuned consumer path per width class: "m k path" lines written by the
+// generator from tuned.json (csrc/generated/variants_index.cu).
+extern const char* const kTunedBatchedPaths[];
+extern const int kTunedBatchedPathCount;
+
+namespace {
+
+// The consumer path of class (m, k): the caller's override when given
+// (class_paths[class] >= 0), else the tuned table's, else the default.
+int class_path(int m, int k, const int* class_paths) {
+  const int cls = batched::class_of(m, k);
+  int path = batched::kPathDefault;
+  if (class_paths != nullptr && class_paths[cls] >= 0) {
+    path = class_paths[cls];
+  } else {
+    for (int i = 0; i < kTunedBatchedPathCount; ++i) {
+      int tm = 0, tk = 0, tp = 0;
+      if (std::sscanf(kTunedBatchedPaths[i], "%d %d %d", &tm, &tk, &tp) == 3 && tm == m && tk == k) path = tp;
+    }
+  }
+  // The SIMT path is the default of the classes below the tensor cores.
+  return batched::dmma_class(m, k) ? path : batched::kPathDefault;
+}
+
 // Cuts the concatenated rows of all problems into one contiguous byte range
 // per CTA (one CTA per SM): CTA b gets bytes [b T / G, (b + 1) T / G).
-tsm_status build_schedule(int count, const tsm_batched_problem_f64* in, int sms, Schedule* out) {
+tsm_status build_schedule(int count, const tsm_batched_problem_f64* in, int sms, Schedule* out,
+                          const int* class_paths = nullptr) {
   if (count < 1 || in == nullptr) return TSM_ERROR_INVALID_VALUE;
+  if (class_paths != nullptr)
+    for (int c = 0; c < 16; ++c)
+      if (class_paths[c] < -1 || class_paths[c] > batched::kPathSimt) return TSM_ERROR_INVALID_VALUE;
   Schedule s;
   s.grid = sms;
   s.problems.resize(count);
@@ -81,9 +111,11 @@ tsm_status build_schedule(int count, const tsm_batched_problem_f64* in, int sms,
     const int cls = batched::class_of(q.m, q.k);
     if (cls < 0) return TSM_ERROR_UNSUPPORTED;  // widths outside {4, 8, 16, 32}
     if (q.n > 0 && (!aligned16(q.A) || !aligned16(q.B))) return TSM_ERROR_UNSUPPORTED;
-    // Tensor-core classes address rows with 32-bit tensor-map coordinates.
-    if (batched::dmma_class(q.m, q.k) && q.n > static_cast<int64_t>(INT_MAX) - 256) return TSM_ERROR_UNSUPPORTED;
+    const int path = class_path(q.m, q.k, class_paths);
+    // The tensor-core path addresses rows with 32-bit tensor-map coordinates.
+    if (batched::uses_dmma(q.m, q.k, path) && q.n > static_cast<int64_t>(INT_MAX) - 256) return TSM_ERROR_UNSUPPORTED;
     BatchedProblemDev& d = s.problems[p];
+    d.path = path;
     d.A = q.A;
     d.B = q.B;
     d.C = q.C;
@@ -179,14 +211,15 @@ size_t tsm_batched_plan_size_f64(int count, const tsm_batched_problem_f64* probl
   return layout(count, static_cast<int>(s.segments.size()), s.grid, s.partial_doubles).total;
 }
 
-tsm_status tsm_batched_plan_init_f64(tsm_stream_t stream, int count, const tsm_batched_problem_f64* problems,
-                                     void* device_buffer, size_t device_bytes, tsm_batched_plan* plan) {
+tsm_status tsm_batched_plan_init_paths_f64(tsm_stream_t stream, int count, const tsm_batched_problem_f64* problems,
+                                           const int* class_paths, void* device_buffer, size_t device_bytes,
+                                           tsm_batched_plan* plan) {
   if (plan == nullptr || device_buffer == nullptr || !aligned16(device_buffer)) return TSM_ERROR_INVALID_VALUE;
   int sms = 0;
   tsm_status st = device_sms(&sms);
   if (st != TSM_SUCCESS) return st;
   Schedule s;
-  if ((st = build_schedule(count, problems, sms, &s)) != TSM_SUCCESS) return st;
+  if ((st = build_schedule(count, problems, sms, &s, class_paths)) != TSM_SUCCESS) return st;
   const int nseg = static_cast<int>(s.segments.size());
   const Layout l = layout(count, nseg, s.grid, s.partial_doubles);
   if (device_bytes < l.total) return TSM_ERROR_WORKSPACE;
@@ -197,14 +230,14 @@ tsm_status tsm_batched_plan_init_f64(tsm_stream_t stream, int count, const tsm_b
   std::memcpy(img.data() + l.problems, s.problems.data(), sizeof(BatchedProblemDev) * count);
   std::memcpy(img.data() + l.segments, s.segments.data(), sizeof(BatchedSegmentDev) * nseg);
   std::memcpy(img.data() + l.cta_first, s.cta_first.data(), sizeof(int) * (s.grid + 1));
-  // Tensor maps of the tensor-core classes: 16-column x rows_of(m, k)-row
+  // Tensor maps of the problems on the tensor-core path: 16-column x rows-row
   // boxes with the 128-byte swizzle the kernel reads with.
   // (Encoded into an aligned local, then copied: the image's bytes carry no
   // 64-byte alignment on the host.)
   for (int p = 0; p < count; ++p) {
     const BatchedProblemDev& d = s.problems[p];
-    if (!batched::dmma_class(d.m, d.k) || d.n == 0) continue;
-    const int rs = batched::rows_of(d.m, d.k);
+    if (!batched::uses_dmma(d.m, d.k, d.path) || d.n == 0) continue;
+    const int rs = batched::rows_of(d.m, d.k, d.path);
     CUtensorMap mp[2];
     if (!encode_rowmajor_map(&mp[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, d.A, d.n, d.m, d.m, 16, rs,
                              CU_TENSOR_MAP_SWIZZLE_128B, &last_error()) ||
@@ -224,6 +257,11 @@ tsm_status tsm_batched_plan_init_f64(tsm_stream_t stream, int count, const tsm_b
   plan->segments = nseg;
   plan->grid = s.grid;
   return TSM_SUCCESS;
+}
+
+tsm_status tsm_batched_plan_init_f64(tsm_stream_t stream, int count, const tsm_batched_problem_f64* problems,
+                                     void* device_buffer, size_t device_bytes, tsm_batched_plan* plan) {
+  return tsm_batched_plan_init_paths_f64(stream, count, problems, nullptr, device_buffer, device_bytes, plan);
 }
 
 tsm_status tsm_gemm_tn_batched_f64(tsm_stream_t stream, const tsm_batched_plan* plan) {

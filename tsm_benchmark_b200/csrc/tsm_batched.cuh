@@ -47,7 +47,7 @@ struct BatchedProblemDev {
   int64_t ldc;
   int64_t seg_first;  // index of the problem's first segment
   int nseg;           // number of segments (>= 1)
-  int pad;
+  int path;           // consumer path of its class: kPathDefault or kPathSimt
 };
 
 struct BatchedSegmentDev {
@@ -83,16 +83,25 @@ constexpr size_t kSmemBytes = kBarOffset + 2 * kStages * sizeof(uint64_t) + 16 +
 // Tensor-core classes: both widths 16 or 32.
 __host__ __device__ constexpr bool dmma_class(int m, int k) { return m >= 16 && k >= 16; }
 
+// Consumer paths.  Every class has its default path (the FP64 tensor cores
+// for the tensor-core classes, SIMT register tiles for the others); the
+// tensor-core classes also have the SIMT path (4 x 4 register tiles over 1-D
+// bulk copies).  The plan picks one per class: the autotuned table, or the
+// caller's override.
+constexpr int kPathDefault = 0;
+constexpr int kPathSimt = 1;
+__host__ __device__ constexpr bool uses_dmma(int m, int k, int path) { return dmma_class(m, k) && path == kPathDefault; }
+
 // 4 x 4 register tiles for every class: sixteen inlined class paths share
 // one register budget, which nine warps per CTA cap at 168 per thread (three
 // warps on one SM sub-partition); larger tiles would spill.
 __host__ __device__ constexpr int tile_of(int) { return 4; }
 
-// Rows per chunk for widths (m, k): ~32 KB stages.  SIMT classes: whole
-// row-group passes.  Tensor-core classes: (m + k) / 16 boxes of 128-byte rows,
-// rows a multiple of 32 (4-row k-steps split evenly over the 8 warps).
-__host__ __device__ constexpr int rows_of(int m, int k) {
-  if (dmma_class(m, k)) return (kStageBytes / (128 * ((m + k) / 16))) / 32 * 32;
+// Rows per chunk for widths (m, k) on a path: ~32 KB stages.  SIMT paths:
+// whole row-group passes.  Tensor-core path: (m + k) / 16 boxes of 128-byte
+// rows, rows a multiple of 32 (4-row k-steps split evenly over the 8 warps).
+__host__ __device__ constexpr int rows_of(int m, int k, int path = kPathDefault) {
+  if (uses_dmma(m, k, path)) return (kStageBytes / (128 * ((m + k) / 16))) / 32 * 32;
   const int nt = (m / tile_of(m)) * (k / tile_of(k));
   const int rg = kCT / nt;
   const int rows = kStageBytes / (8 * (m + k));
@@ -153,7 +162,7 @@ __device__ __forceinline__ void consume_segment(const BatchedArgs& a, const Batc
   constexpr int TA = tile_of(M), TB = tile_of(K);
   using S = TileShape<M, K, TA, TB>;
   constexpr int RG = kCT / S::NT;
-  constexpr int RS = rows_of(M, K);
+  constexpr int RS = rows_of(M, K, kPathSimt);
   constexpr int EPC = 2;
   constexpr bool VEC_A = TA % EPC == 0, VEC_B = TB % EPC == 0;
   constexpr int NCH_A = TA / EPC, NCH_B = TB / EPC;
@@ -329,8 +338,8 @@ __global__ void __launch_bounds__(batched::kThreads, 1) tsm_tn_batched_kernel(co
     for (int si = first; si < last && ok; ++si) {
       const BatchedSegmentDev seg = a.segments[si];
       const BatchedProblemDev& pr = a.problems[seg.problem];
-      const int rs = rows_of(pr.m, pr.k);
-      const bool tc = dmma_class(pr.m, pr.k);
+      const int rs = rows_of(pr.m, pr.k, pr.path);
+      const bool tc = uses_dmma(pr.m, pr.k, pr.path);
       const CUtensorMap* ta = a.maps + 2 * seg.problem;
       if (tc && lane == 0 && seg.r1 > seg.r0) {
         dev::fence_tensormap_acquire(ta);
@@ -380,7 +389,10 @@ __global__ void __launch_bounds__(batched::kThreads, 1) tsm_tn_batched_kernel(co
     break;
 #define TSM_BATCHED_TC_CASE(M, K)                                                                       \
   case class_of(M, K):                                                                                  \
-    consume_segment_dmma<M, K>(a, seg, pr, ring, red, full, empty, abort, s_flag, it, t);               \
+    if (pr.path == kPathSimt)                                                                           \
+      consume_segment<M, K>(a, seg, pr, ring, red, full, empty, abort, s_flag, it, t);                  \
+    else                                                                                                \
+      consume_segment_dmma<M, K>(a, seg, pr, ring, red, full, empty, abort, s_flag, it, t);             \
     break;
       switch (pr.cls) {
         TSM_BATCHED_CASE(4, 4) TSM_BATCHED_CASE(4, 8) TSM_BATCHED_CASE(4, 16) TSM_BATCHED_CASE(4, 32)
@@ -402,7 +414,7 @@ __global__ void __launch_bounds__(batched::kThreads, 1) tsm_tn_batched_kernel(co
     for (int si = first; si < last; ++si) {
       const BatchedSegmentDev seg = a.segments[si];
       const BatchedProblemDev& pr = a.problems[seg.problem];
-      const int rs = rows_of(pr.m, pr.k);
+      const int rs = rows_of(pr.m, pr.k, pr.path);
       issued += (seg.r1 - seg.r0 + rs - 1) / rs;
     }
     volatile int no_abort = 0;

@@ -258,7 +258,8 @@ tsm_status launch_variant(const Variant* v, const PlainArgs<T>& p, int64_t grid,
 
 template <typename T>
 tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const T* A, int64_t lda, const T* B,
-                        int64_t ldb, T* C, int64_t ldc, int accumulate, void* ws, size_t ws_bytes, int variant) {
+                        int64_t ldb, T* C, int64_t ldc, int accumulate, void* ws, size_t ws_bytes, int variant,
+                        int64_t max_ctas = 0) {
   constexpr int dtype = DTypeOf<T>::value;
   tsm_status s = check_args(n, m, k, A, lda, B, ldb, C, ldc);
   if (s != TSM_SUCCESS) return s;
@@ -295,7 +296,8 @@ tsm_status launch_plain(cudaStream_t stream, int64_t n, int m, int k, const T* A
   p.error = reinterpret_cast<unsigned*>(base) + 1;
   p.partials = reinterpret_cast<double*>(base + kWsHeader);
 
-  const int64_t grid = plan_grid(v, st, idx, p);
+  int64_t grid = plan_grid(v, st, idx, p);
+  if (max_ctas > 0) grid = std::min(grid, max_ctas);  // every kernel deals its rows over any grid >= 1
   return launch_variant(v, p, grid, stream);
 }
 
@@ -378,6 +380,13 @@ tsm_status tsm_gemm_tn_f64_variant(tsm_stream_t stream, int64_t n, int m, int k,
                                    void* workspace, size_t workspace_bytes, int variant) {
   return launch_plain<double>(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate,
                               workspace, workspace_bytes, variant);
+}
+
+tsm_status tsm_gemm_tn_f64_launch(tsm_stream_t stream, int64_t n, int m, int k, const double* A, int64_t lda,
+                                  const double* B, int64_t ldb, double* C, int64_t ldc, int accumulate,
+                                  void* workspace, size_t workspace_bytes, int variant, int64_t max_ctas) {
+  return launch_plain<double>(static_cast<cudaStream_t>(stream), n, m, k, A, lda, B, ldb, C, ldc, accumulate,
+                              workspace, workspace_bytes, variant, max_ctas);
 }
 
 tsm_status tsm_gemm_tn_f32(tsm_stream_t stream, int64_t n, int m, int k, const float* A, int64_t lda,
