@@ -75,6 +75,9 @@ def lib() -> ctypes.CDLL:
         L.tsm_oracle_dot2_uniform.argtypes = [I64, I64, I, I, ctypes.c_uint64, P, P, P, P]
         L.tsm_oracle_dot2_uniform.restype = I
         L.tsm_oracle_force_split.argtypes = [I]
+        L.tsm_oracle_dot2_uniform_ex.argtypes = [I64, I64, I64, I, I, ctypes.c_uint64, ctypes.c_uint64,
+                                                 ctypes.c_uint64, I, P, P, P, P]
+        L.tsm_oracle_dot2_uniform_ex.restype = I
         _lib = L
     return _lib
 
@@ -226,10 +229,18 @@ class Dot2Stream:
             raise MemoryError("oracle: host buffers")
         self.rows += n
 
-    def add_uniform(self, seed: int, row0: int, rows: int) -> None:
-        """Rows [row0, row0 + rows) of operands(n, m, k, seed)'s values."""
-        rc = lib().tsm_oracle_dot2_uniform(row0, rows, self.m, self.k, seed, _p(self.S), _p(self.E), _p(self.nrm),
-                                           self._abs())
+    def add_uniform(self, seed: int, row0: int, rows: int, *, streams: tuple[int, int] = (0, 1),
+                    col_major_n: int = 0) -> None:
+        """Rows [row0, row0 + rows) of counter-based uniform operands: A from
+        streams[0], B from streams[1] (equal streams and m == k: B is A).
+        Row-major by default (operands(n, m, k, seed)'s values); with
+        col_major_n = n, the values fill_uniform writes into A^T and B^T
+        stored row-major (m x n and k x n)."""
+        if streams[0] == streams[1] and self.m != self.k:
+            raise ValueError("B is A only for m == k")
+        rc = lib().tsm_oracle_dot2_uniform_ex(row0, rows, col_major_n or (row0 + rows), self.m, self.k, seed,
+                                              streams[0], streams[1], 1 if col_major_n else 0, _p(self.S),
+                                              _p(self.E), _p(self.nrm), self._abs())
         if rc != 0:
             raise MemoryError("oracle: host buffers")
         self.rows += rows
@@ -244,9 +255,11 @@ class Dot2Stream:
         return out
 
 
-def dot2_uniform(n: int, m: int, k: int, seed: int, with_abs: bool = False) -> dict:
+def dot2_uniform(n: int, m: int, k: int, seed: int, with_abs: bool = False, *, gram: bool = False,
+                 col_major: bool = False) -> dict:
     """Dot2Stream over all n rows of operands(n, m, k, seed), generated on
-    the host as it goes."""
+    the host as it goes; gram: B is A (stream 0); col_major: the values of
+    A^T, B^T filled row-major."""
     d = Dot2Stream(m, k, with_abs)
-    d.add_uniform(seed, 0, n)
+    d.add_uniform(seed, 0, n, streams=(0, 0) if gram else (0, 1), col_major_n=n if col_major else 0)
     return d.result()

@@ -387,8 +387,10 @@ static int host_has_fma(void) {
 EXPORT void tsm_oracle_force_split(int on) { g_force_split = on; }
 
 /* Where a block's values come from: host arrays (FP64 or FP32, row pitches
- * lda, ldb), or the counter-based uniform generator (A = stream 0, B =
- * stream 1 under `seed`, contiguous: element (r, i) of A is value r*m + i). */
+ * lda, ldb), or the counter-based uniform generator (A from stream sa, B
+ * from stream sb under `seed`; row-major: element (r, i) of A is value
+ * r*m + i of its stream; column-major, the layout of A^T stored row-major
+ * with pitch n_total: value i*n_total + r). */
 typedef struct {
   const void* A;
   const void* B;
@@ -397,19 +399,31 @@ typedef struct {
   int generate;
   uint64_t seed;
   int64_t row0; /* global index of row 0 of this call (generator) */
+  uint64_t sa, sb;
+  int col_major;
+  int64_t n_total;
 } dot2_source;
+
+static inline double uniform_at(uint64_t seed, uint64_t stream, uint64_t idx) {
+  return 2.0 * ((double)(splitmix64_at(seed, stream, idx) >> 11) * 0x1.0p-53) - 1.0;
+}
+
+static void gen_block(const dot2_source* src, uint64_t stream, int w, int64_t r, int64_t rows, double* x) {
+  const int64_t g = src->row0 + r; /* global first row of the block */
+  if (!src->col_major) {
+    for (int64_t q = 0; q < rows * w; ++q) x[q] = uniform_at(src->seed, stream, (uint64_t)(g * w + q));
+    return;
+  }
+  for (int i = 0; i < w; ++i)
+    for (int64_t q = 0; q < rows; ++q)
+      x[q * w + i] = uniform_at(src->seed, stream, (uint64_t)((int64_t)i * src->n_total + g + q));
+}
 
 static void dot2_load(const dot2_source* src, int m, int k, int64_t r, int64_t rows, double* a,
                       double* b) {
   if (src->generate) {
-    for (int64_t q = 0; q < rows * m; ++q) {
-      const uint64_t idx = (uint64_t)((src->row0 + r) * m) + (uint64_t)q;
-      a[q] = 2.0 * ((double)(splitmix64_at(src->seed, 0, idx) >> 11) * 0x1.0p-53) - 1.0;
-    }
-    for (int64_t q = 0; q < rows * k; ++q) {
-      const uint64_t idx = (uint64_t)((src->row0 + r) * k) + (uint64_t)q;
-      b[q] = 2.0 * ((double)(splitmix64_at(src->seed, 1, idx) >> 11) * 0x1.0p-53) - 1.0;
-    }
+    gen_block(src, src->sa, m, r, rows, a);
+    gen_block(src, src->sb, k, r, rows, b);
     return;
   }
   for (int64_t q = 0; q < rows; ++q) {
@@ -498,16 +512,26 @@ static int dot2_stream(const dot2_source* src, int64_t rows, int m, int k, doubl
 EXPORT int tsm_oracle_dot2_acc(int64_t rows, int m, int k, const void* A, int64_t lda, const void* B,
                                int64_t ldb, int f32, double* S, double* E, double* nrm, double* absC) {
   if (rows <= 0) return 0;
-  dot2_source src = {A, B, lda, ldb, f32, 0, 0, 0};
+  dot2_source src = {A, B, lda, ldb, f32, 0, 0, 0, 0, 0, 0, 0};
   return dot2_stream(&src, rows, m, k, S, E, nrm, absC);
 }
 
-/* The same over the counter-based uniform operands of `seed` (A = stream 0,
- * B = stream 1, contiguous, rows [row0, row0 + rows)): the values the
- * library's device fill writes, generated block by block on the host. */
+/* The same over counter-based uniform operands of `seed`: A from stream sa,
+ * B from stream sb (sb == sa with k == m: B is A, the Gram product), rows
+ * [row0, row0 + rows) of an n_total-row operand pair, row-major (contiguous)
+ * or column-major (A^T stored row-major with pitch n_total): the values the
+ * library's device fill writes into those buffers, generated block by block
+ * on the host. */
+EXPORT int tsm_oracle_dot2_uniform_ex(int64_t row0, int64_t rows, int64_t n_total, int m, int k,
+                                      uint64_t seed, uint64_t sa, uint64_t sb, int col_major, double* S,
+                                      double* E, double* nrm, double* absC) {
+  if (rows <= 0) return 0;
+  dot2_source src = {NULL, NULL, 0, 0, 0, 1, seed, row0, sa, sb, col_major, n_total};
+  return dot2_stream(&src, rows, m, k, S, E, nrm, absC);
+}
+
+/* Row-major operands, A = stream 0, B = stream 1: oracle.operands' values. */
 EXPORT int tsm_oracle_dot2_uniform(int64_t row0, int64_t rows, int m, int k, uint64_t seed, double* S,
                                    double* E, double* nrm, double* absC) {
-  if (rows <= 0) return 0;
-  dot2_source src = {NULL, NULL, 0, 0, 0, 1, seed, row0};
-  return dot2_stream(&src, rows, m, k, S, E, nrm, absC);
+  return tsm_oracle_dot2_uniform_ex(row0, rows, row0 + rows, m, k, seed, 0, 1, 0, S, E, nrm, absC);
 }

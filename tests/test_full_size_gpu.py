@@ -15,7 +15,9 @@ are checked against the oracle, not against another GPU library:
 * split precision: the FP32 operands are copied to the host in row chunks
   and fed to the same compensated product; acceptance is the stated error of
   each kind, normwise and per entry relative to sum_r |a_ri| |b_rj|.
-* differentiation: dA = B dC^T and dB = A dC against the oracle's TSMM.
+* differentiation: dA = B dC^T and dB = A dC against the oracle's TSMM;
+* the Gram product and column-major operands at their benchmark sizes, the
+  oracle regenerating A alone, or the values written into A^T and B^T.
 """
 import numpy as np
 import pytest
@@ -133,3 +135,48 @@ def test_autograd_config_backward_against_oracle(gpu, oracle_mod, dtype):
         assert rel <= tol, (dtype, rel, tol)
     del dA, dB
     _free()
+
+
+GRAM = [(1 << 26, 8), (1 << 26, 32), (1 << 23, 64)]
+
+
+@pytest.mark.parametrize("n,m", GRAM, ids=[f"2^{n.bit_length() - 1}x{m}" for n, m in GRAM])
+def test_gram_at_benchmark_size_against_oracle(gpu, oracle_mod, n, m):
+    """C = A^T A (A streamed once, upper triangle) at the Gram benchmark's
+    sizes: the exact normwise bound against the oracle, and C exactly
+    symmetric."""
+    from tsm_benchmark_b200 import fill_uniform, gram
+    seed = 77 + m
+    A = torch.empty((n, m), dtype=torch.float64, device=gpu)
+    fill_uniform(A, seed, 0)
+    got = gram(A).cpu().numpy()
+    del A
+    _free()
+    assert np.array_equal(got, got.T)
+    ref = oracle_mod.dot2_uniform(n, m, m, seed, gram=True)
+    err = float(np.linalg.norm(got - ref["C"]))
+    assert err <= ref["bound"], (n, m, err, ref["bound"])
+    assert oracle_mod.check(ref["C"], got, REL_TOL, ABS_TOL) == -1
+
+
+COLUMN_MAJOR = [(1 << 26, 8, 8), (1 << 25, 4, 32), (1 << 25, 32, 32), (1 << 23, 64, 64)]
+
+
+@pytest.mark.parametrize("n,m,k", COLUMN_MAJOR, ids=[f"2^{n.bit_length() - 1}x{m}x{k}" for n, m, k in COLUMN_MAJOR])
+def test_column_major_at_benchmark_size_against_oracle(gpu, oracle_mod, n, m, k):
+    """Column-major operands (A^T, B^T stored row-major, read in place by
+    the tensor-map kernels) at the column-major benchmark's sizes, against
+    the oracle at the exact bound."""
+    from tsm_benchmark_b200 import fill_uniform, tsmttsm
+    seed = 91 + m + k
+    At = torch.empty((m, n), dtype=torch.float64, device=gpu)
+    Bt = torch.empty((k, n), dtype=torch.float64, device=gpu)
+    fill_uniform(At, seed, 0)
+    fill_uniform(Bt, seed, 1)
+    got = tsmttsm(At.t(), Bt.t()).cpu().numpy()
+    del At, Bt
+    _free()
+    ref = oracle_mod.dot2_uniform(n, m, k, seed, col_major=True)
+    err = float(np.linalg.norm(got - ref["C"]))
+    assert err <= ref["bound"], (n, m, k, err, ref["bound"])
+    assert oracle_mod.check(ref["C"], got, REL_TOL, ABS_TOL) == -1

@@ -223,3 +223,20 @@ def test_streaming_dot2_decides_between_naive_and_blocked_sums(oracle_mod):
     naive = oracle_mod.naive(A, B)
     assert np.linalg.norm(naive - ref["C"]) <= ref["bound"]
     assert np.all(np.abs(ref["C"] - oracle_mod.dot2(A, B)) <= np.spacing(np.abs(ref["C"])))
+
+
+def test_streaming_dot2_gram_and_column_major_generation(oracle_mod):
+    """The streaming oracle's other generated layouts: B is A (same stream),
+    and column-major operands (the values a fill of A^T, B^T writes),
+    against the compensated product of explicitly built host arrays."""
+    n, m, k = 3001, 5, 7
+    A, _ = oracle_mod.operands(n, m, k, 9)
+    assert np.array_equal(oracle_mod.dot2_uniform(n, m, m, 9, gram=True)["C"], oracle_mod.dot2(A, A))
+    At = oracle_mod.uniform(m * n, 9, 0).reshape(m, n)
+    Bt = oracle_mod.uniform(k * n, 9, 1).reshape(k, n)
+    ref = oracle_mod.dot2(np.ascontiguousarray(At.T), np.ascontiguousarray(Bt.T))
+    assert np.array_equal(oracle_mod.dot2_uniform(n, m, k, 9, col_major=True)["C"], ref)
+    d = oracle_mod.Dot2Stream(m, k)
+    d.add_uniform(9, 0, 1000, col_major_n=n)
+    d.add_uniform(9, 1000, n - 1000, col_major_n=n)
+    assert np.array_equal(d.result()["C"], ref)
