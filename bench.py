@@ -385,14 +385,20 @@ def forms(dev) -> dict:
         B = (torch.rand((n, w), device=dev, generator=g, dtype=torch.float64) * 2 - 1).to(dt)
         Wl = torch.randn((w, w), device=dev, generator=g, dtype=torch.float64).to(dt)
         C = torch.empty((w, w), dtype=dt, device=dev)
-        ms_fwd = _time(lambda: tsm.tsmttsm(A, B, C), 50)
-        ms_bwd = _time(lambda: tsm.tsmttsm_backward(A, B, Wl), 50)
+        ms_fwd = _time(lambda: tsm.tsmttsm(A, B, C), 50, warmup=20)
+        ms_bwd = _time(lambda: tsm.tsmttsm_backward(A, B, Wl), 50, warmup=20)
+        # The backward's read + write roof: a device-to-device copy of the
+        # same bytes (A -> dA-sized, B -> dB-sized buffers).
+        dA_, dB_ = torch.empty_like(A), torch.empty_like(B)
+        ms_copy = _time(lambda: (dA_.copy_(A), dB_.copy_(B)), 50, warmup=20)
         esz = A.element_size()
         out[name] = {"n": n, "m": w, "k": w, "fwd_ms": round(ms_fwd, 4), "bwd_ms": round(ms_bwd, 4),
                      "bwd_over_fwd": round(ms_bwd / ms_fwd, 3),
                      "fwd_GB/s": round(esz * n * 2 * w / (ms_fwd * 1e-3) / 1e9, 1),
-                     "bwd_GB/s": round(2 * esz * n * 2 * w / (ms_bwd * 1e-3) / 1e9, 1)}
-        del A, B
+                     "bwd_GB/s": round(2 * esz * n * 2 * w / (ms_bwd * 1e-3) / 1e9, 1),
+                     "d2d_copy_same_bytes_ms": round(ms_copy, 4),
+                     "bwd_over_copy": round(ms_bwd / ms_copy, 3)}
+        del A, B, dA_, dB_
         torch.cuda.empty_cache()
     return out
 
@@ -661,7 +667,8 @@ def summary(line: dict) -> str:
     for key in ("autograd_f64", "autograd_f32"):
         if key in f:
             x = f[key]
-            out.append(f"  {key}: fwd {x['fwd_ms']} ms, bwd {x['bwd_ms']} ms ({x['bwd_over_fwd']}x)")
+            out.append(f"  {key}: fwd {x['fwd_ms']} ms, bwd {x['bwd_ms']} ms ({x['bwd_over_fwd']}x; "
+                       f"{x['bwd_over_copy']}x a D2D copy of the same bytes)")
     if line.get("cpu_baseline"):
         c = line["cpu_baseline"]
         out.append(f"cpu baseline ({c['kind']}, {c['cores']} cores): {c['value']:.3f} GB/s; {c['sample']}")
