@@ -3,8 +3,8 @@
 //
 // Same arithmetic as tsm_split.cuh -- x = hi + lo with two TF32 parts, one
 // tcgen05.mma (kind::tf32, M = 64 = [A_hi ; A_lo], N = 64 = [B_hi | B_lo],
-// K = 8 rows) per 8 rows, FP32 accumulation in tensor memory for 128 rows,
-// FP64 beyond -- with a leaner data path:
+// K = 8 rows) per 8 rows, FP32 accumulation in tensor memory for DRAIN
+// chunks of one issuer, FP64 beyond -- with a leaner data path:
 //   * the producer loads 128-row chunks of A and B with 2-D tiled TMA
 //     (tensor maps with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, box 32 columns x
 //     128 rows): the raw FP32 tile lands directly in the MN-major layout that
@@ -55,31 +55,38 @@ struct SplitTmaArgs {
 
 namespace split2 {
 
-constexpr int kRows = 128;                   // rows per chunk (16 MMAs of K = 8)
-// kIssuers warps issue the MMAs (chunk it goes to issuer it % kIssuers);
-// each owns one lo stage and one TMEM accumulator.
-constexpr int kIssuers = 3;
-constexpr int kHiStages = kIssuers == 2 ? 5 : kIssuers == 3 ? 4 : 3;
-constexpr int kLoStages = kIssuers;
-constexpr int kTileBytes = kRows * 128;      // one operand part: 32 floats x 128 rows
-constexpr int kStageBytes = 2 * kTileBytes;  // A part, B part
-constexpr int kLoRing = kHiStages * kStageBytes;  // offset of the lo ring
-constexpr int kConvWarps = 8;
-constexpr int kConvWarp0 = 1 + kIssuers;           // warps: 0 producer, 1 .. kIssuers issuers,
-constexpr int kEpiWarp0 = kConvWarp0 + kConvWarps;  // then converters, then 4 epilogue warps
-constexpr int kWarps = kEpiWarp0 + 4;
-constexpr int kConvJobs = 2 * kTileBytes / 16 / (32 * kConvWarps);  // 16-byte vectors per converter thread
-static_assert(kConvJobs * 32 * kConvWarps * 16 == 2 * kTileBytes, "converters cover the stage exactly");
-constexpr int kThreads = kWarps * 32;
-constexpr int kTmemCols = kIssuers * 64 <= 128 ? 128 : 256;  // one 64-column accumulator per issuer
+// Constants of the kernel for chunks of ROWS rows (ROWS / 8 MMAs of K = 8).
+template <int ROWS>
+struct Cfg {
+  static constexpr int kRows = ROWS;
+  // kIssuers warps issue the MMAs (chunk it goes to issuer it % kIssuers);
+  // each owns one lo stage and one TMEM accumulator.
+  static constexpr int kIssuers = 3;
+  static constexpr int kTileBytes = kRows * 128;      // one operand part: 32 floats x kRows rows
+  static constexpr int kStageBytes = 2 * kTileBytes;  // A part, B part
+  static constexpr int kLoStages = kIssuers;
+  // hi and lo stages share 224 KB: 4 hi stages of 128 rows, 11 of 64 rows
+  static constexpr int kHiStages = (7 * 32768) / kStageBytes - kLoStages;
+  static constexpr int kLoRing = kHiStages * kStageBytes;  // offset of the lo ring
+  static constexpr int kConvWarps = 8;
+  static constexpr int kConvWarp0 = 1 + kIssuers;           // warps: 0 producer, 1 .. kIssuers issuers,
+  static constexpr int kEpiWarp0 = kConvWarp0 + kConvWarps;  // then converters, then 4 epilogue warps
+  static constexpr int kWarps = kEpiWarp0 + 4;
+  static constexpr int kConvJobs = 2 * kTileBytes / 16 / (32 * kConvWarps);  // 16-byte vectors per converter thread
+  static constexpr int kThreads = kWarps * 32;
+  static constexpr int kTmemCols = kIssuers * 64 <= 128 ? 128 : 256;  // one 64-column accumulator per issuer
+  static constexpr size_t kBarOffset = size_t(kLoRing) + size_t(kLoStages) * kStageBytes;
+  static constexpr int kNumBars = 2 * kHiStages + 2 * kLoStages + 2 * kIssuers;
+  static constexpr size_t kSmemBytes = kBarOffset + kNumBars * 8 + 32 + 1024;  // + alignment slack
+  static_assert(kHiStages >= 2, "at least a double-buffered hi ring");
+  static_assert(kConvJobs * 32 * kConvWarps * 16 == 2 * kTileBytes, "converters cover the stage exactly");
+  static_assert(kTileBytes % 1024 == 0, "tiles keep the 1024-byte alignment of the swizzle atoms");
+  static_assert((kLoRing + (kLoStages - 1) * kStageBytes) / 16 < (1 << 14), "LBO must fit the descriptor field");
+  static_assert(kSmemBytes <= 232448, "dynamic shared memory limit of sm_100a");
+  static_assert(kWarps <= 16, "17 warps cap registers at 96 a thread and spill the epilogue sums");
+};
+
 constexpr uint32_t kIdesc = dev::umma_idesc_tf32(64, 64, true, true);
-constexpr size_t kBarOffset = size_t(kLoRing) + size_t(kLoStages) * kStageBytes;
-constexpr int kNumBars = 2 * kHiStages + 2 * kLoStages + 2 * kIssuers;
-constexpr size_t kSmemBytes = kBarOffset + kNumBars * 8 + 32 + 1024;  // + alignment slack
-static_assert(kTileBytes % 1024 == 0, "tiles keep the 1024-byte alignment of the swizzle atoms");
-static_assert((kLoRing + (kLoStages - 1) * kStageBytes) / 16 < (1 << 14), "LBO must fit the descriptor field");
-static_assert(kSmemBytes <= 232448, "dynamic shared memory limit of sm_100a");
-static_assert(kWarps <= 16, "17 warps cap registers at 96 a thread and spill the epilogue sums");
 
 // lo part of x: x - trunc_tf32(x) (exact) rounded to nearest TF32, ties away
 // from zero (add half a TF32 unit to the magnitude bits, clear 13 bits).
@@ -92,9 +99,21 @@ __device__ __forceinline__ uint32_t lo_part(uint32_t xb) {
 
 }  // namespace split2
 
-__global__ void __launch_bounds__(split2::kThreads, 1)
+// DRAIN: chunks of one issuer accumulated in its TMEM accumulator before the
+// epilogue drains it (FP32 accumulation over DRAIN * ROWS rows).
+template <int ROWS, int DRAIN>
+__global__ void __launch_bounds__(split2::Cfg<ROWS>::kThreads, 1)
     tsm_tn_split_tf32_tma_kernel(const __grid_constant__ SplitTmaArgs args) {
-  using namespace split2;
+  using S = split2::Cfg<ROWS>;
+  static_assert(DRAIN >= 1, "at least one chunk per drain");
+  using split2::kIdesc;
+  using split2::lo_part;
+  constexpr int kRows = S::kRows, kIssuers = S::kIssuers, kTileBytes = S::kTileBytes;
+  constexpr int kStageBytes = S::kStageBytes, kLoStages = S::kLoStages, kHiStages = S::kHiStages;
+  constexpr int kLoRing = S::kLoRing, kConvWarps = S::kConvWarps, kConvWarp0 = S::kConvWarp0;
+  constexpr int kEpiWarp0 = S::kEpiWarp0, kConvJobs = S::kConvJobs, kThreads = S::kThreads;
+  constexpr int kTmemCols = S::kTmemCols, kNumBars = S::kNumBars;
+  constexpr size_t kBarOffset = S::kBarOffset;
   const SplitArgs& p = args.p;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((1024u - (dev::smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -140,6 +159,12 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
 
   int64_t nchunks_mine = 0;
   for (int64_t c = blockIdx.x; c < p.num_chunks; c += G) ++nchunks_mine;
+  // Chunk it belongs to issuer (and accumulator) it % kIssuers, as that
+  // issuer's chunk j = it / kIssuers, in drain group j / DRAIN; the group's
+  // last chunk (or the issuer's last) hands the accumulator to the epilogue.
+  auto ends_group = [&](int64_t it) {
+    return (it / kIssuers) % DRAIN == DRAIN - 1 || it + kIssuers >= nchunks_mine;
+  };
 
   double acc[32];
 #pragma unroll
@@ -181,11 +206,13 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       const int s = static_cast<int>(it % kHiStages);
       const int o = static_cast<int>(it % kLoStages);
       const int b = static_cast<int>(it % kIssuers);
+      const int64_t j = it / kIssuers, grp = j / DRAIN;
+      const bool group_first = j % DRAIN == 0;
       bool ok = true;
       if (lane == 0) {
         ok = dev::mbar_wait(&lo_full[o], static_cast<uint32_t>((it / kLoStages) & 1), abort);
-        if (ok && it >= kIssuers)
-          ok = dev::mbar_wait(&d_empty[b], static_cast<uint32_t>(((it / kIssuers) - 1) & 1), abort);
+        if (ok && group_first && grp > 0)
+          ok = dev::mbar_wait(&d_empty[b], static_cast<uint32_t>((grp - 1) & 1), abort);
         if (ok) {
           dev::tc_fence_after();
           const uint32_t a_base = base + s * kStageBytes;
@@ -195,11 +222,11 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
           for (int g = 0; g < kRows / 8; ++g) {
             const uint64_t ad = dev::umma_smem_desc(a_base + g * 1024, lbo, split::kSbo, split::kLayout);
             const uint64_t bd = dev::umma_smem_desc(b_base + g * 1024, lbo, split::kSbo, split::kLayout);
-            dev::umma_tf32(tmem + b * 64, ad, bd, kIdesc, g > 0 ? 1u : 0u);
+            dev::umma_tf32(tmem + b * 64, ad, bd, kIdesc, (g > 0 || !group_first) ? 1u : 0u);
           }
           dev::umma_commit(&empty[s]);     // the hi stage may be refilled once these MMAs are done
           dev::umma_commit(&lo_empty[o]);  // and the lo stage rewritten
-          dev::umma_commit(&d_full[b]);
+          if (ends_group(it)) dev::umma_commit(&d_full[b]);
         } else {
           *abort = 1;
           atomicOr(p.error, dev::kErrTimeout);
@@ -244,8 +271,9 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
     const int q = warp & 3;
     const uint32_t lane_base = static_cast<uint32_t>(32 * q) << 16;
     for (int64_t it = 0; it < nchunks_mine; ++it) {
+      if (!ends_group(it)) continue;
       const int b = static_cast<int>(it % kIssuers);
-      if (!dev::mbar_wait(&d_full[b], static_cast<uint32_t>((it / kIssuers) & 1), abort)) {
+      if (!dev::mbar_wait(&d_full[b], static_cast<uint32_t>(((it / kIssuers) / DRAIN) & 1), abort)) {
         *abort = 1;
         atomicOr(p.error, dev::kErrTimeout);
         break;
@@ -278,8 +306,11 @@ __global__ void __launch_bounds__(split2::kThreads, 1)
       for (int64_t it = nchunks_mine > kHiStages ? nchunks_mine - kHiStages : 0; it < nchunks_mine; ++it)
         if (!dev::mbar_wait(&full[it % kHiStages], static_cast<uint32_t>((it / kHiStages) & 1), &no_abort)) break;
     } else if (warp == 1) {
-      for (int64_t it = nchunks_mine > kIssuers ? nchunks_mine - kIssuers : 0; it < nchunks_mine; ++it)
-        if (!dev::mbar_wait(&d_full[it % kIssuers], static_cast<uint32_t>((it / kIssuers) & 1), &no_abort)) break;
+      const int64_t span = int64_t(kIssuers) * DRAIN;
+      for (int64_t it = nchunks_mine > span ? nchunks_mine - span : 0; it < nchunks_mine; ++it)
+        if (ends_group(it) && !dev::mbar_wait(&d_full[it % kIssuers],
+                                              static_cast<uint32_t>(((it / kIssuers) / DRAIN) & 1), &no_abort))
+          break;
     }
   }
   dev::tc_fence_before();
