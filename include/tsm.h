@@ -309,7 +309,7 @@ typedef struct tsm_batched_plan {
   int count;
   int segments;
   int grid;
-  int reserved;
+  int flags;  /* set by the plan init: 1 when a tensor-core class runs its SIMT path */
 } tsm_batched_plan;
 
 /* Device bytes the plan for these problems needs on the current device

@@ -120,7 +120,11 @@ def test_batched_both_paths_of_the_tensor_core_classes(gpu, oracle_mod, path):
         Bs.append(torch.from_numpy(B).to(gpu))
         host.append((A, B))
     paths = {(m, k): path for m in (16, 32) for k in (16, 32)}
-    Cs = BatchedTSMTTSM(As, Bs, class_paths=paths).run()
+    bt = BatchedTSMTTSM(As, Bs, class_paths=paths)
+    # the plan runs the kernel instantiation with the SIMT tensor-core paths
+    # only when a class was sent down one
+    assert bt.plan.flags == (1 if path == "simt" else 0)
+    Cs = bt.run()
     torch.cuda.synchronize()
     for i, ((A, B), C) in enumerate(zip(host, Cs)):
         ref = oracle_mod.naive(A, B)

@@ -63,7 +63,7 @@ class BatchedProblem(ctypes.Structure):
 
 class BatchedPlan(ctypes.Structure):
     _fields_ = [("device", c_void_p), ("bytes", c_size_t), ("count", c_int), ("segments", c_int),
-                ("grid", c_int), ("reserved", c_int)]
+                ("grid", c_int), ("flags", c_int)]
 
 
 # Every function declared in include/tsm.h: name -> (restype, argtypes).

@@ -187,9 +187,11 @@ tsm_status device_sms(int* sms) {
     if (e != cudaSuccess) return fail(e, "cudaDeviceGetAttribute");
   }
   if (!g_attr[dev]) {
-    e = cudaFuncSetAttribute(reinterpret_cast<const void*>(&tsm_tn_batched_kernel),
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(batched::kSmemBytes));
-    if (e != cudaSuccess) return fail(e, "cudaFuncSetAttribute(batched)");
+    for (const void* fn : {reinterpret_cast<const void*>(&tsm_tn_batched_kernel<false>),
+                           reinterpret_cast<const void*>(&tsm_tn_batched_kernel<true>)}) {
+      e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(batched::kSmemBytes));
+      if (e != cudaSuccess) return fail(e, "cudaFuncSetAttribute(batched)");
+    }
     g_attr[dev] = true;
   }
   *sms = g_sms[dev];
@@ -256,6 +258,9 @@ tsm_status tsm_batched_plan_init_paths_f64(tsm_stream_t stream, int count, const
   plan->count = count;
   plan->segments = nseg;
   plan->grid = s.grid;
+  plan->flags = 0;
+  for (const BatchedProblemDev& d : s.problems)
+    if (batched::dmma_class(d.m, d.k) && d.path == batched::kPathSimt) plan->flags = 1;
   return TSM_SUCCESS;
 }
 
@@ -282,7 +287,9 @@ tsm_status tsm_gemm_tn_batched_f64(tsm_stream_t stream, const tsm_batched_plan* 
   a.partials = reinterpret_cast<double*>(base + l.partials);
   a.error = reinterpret_cast<unsigned*>(base) + 1;
   void* args[] = {&a};
-  const cudaError_t e = cudaLaunchKernel(reinterpret_cast<const void*>(&tsm_tn_batched_kernel), dim3(plan->grid),
+  const void* fn = plan->flags ? reinterpret_cast<const void*>(&tsm_tn_batched_kernel<true>)
+                               : reinterpret_cast<const void*>(&tsm_tn_batched_kernel<false>);
+  const cudaError_t e = cudaLaunchKernel(fn, dim3(plan->grid),
                                          dim3(batched::kThreads), args, batched::kSmemBytes,
                                          static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return fail(e, "cudaLaunchKernel(batched)");

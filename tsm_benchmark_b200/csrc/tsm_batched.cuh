@@ -306,6 +306,10 @@ __device__ __forceinline__ void consume_segment_dmma(const BatchedArgs& a, const
 
 }  // namespace batched
 
+// SIMT_TC: the tensor-core classes may take their SIMT path (a plan that
+// overrides one uses this instantiation; the default one leaves those paths
+// out, which measured 1-5 % faster for the 512-problem batch).
+template <bool SIMT_TC>
 __global__ void __launch_bounds__(batched::kThreads, 1) tsm_tn_batched_kernel(const BatchedArgs a) {
   using namespace batched;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -389,7 +393,7 @@ __global__ void __launch_bounds__(batched::kThreads, 1) tsm_tn_batched_kernel(co
     break;
 #define TSM_BATCHED_TC_CASE(M, K)                                                                       \
   case class_of(M, K):                                                                                  \
-    if (pr.path == kPathSimt)                                                                           \
+    if (SIMT_TC && pr.path == kPathSimt)                                                                \
       consume_segment<M, K>(a, seg, pr, ring, red, full, empty, abort, s_flag, it, t);                  \
     else                                                                                                \
       consume_segment_dmma<M, K>(a, seg, pr, ring, red, full, empty, abort, s_flag, it, t);             \
