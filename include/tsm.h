@@ -133,7 +133,7 @@ tsm_status tsm_gemm_tn_f32_split(tsm_stream_t stream, int64_t n, int m, int k, c
  * h = rn(x) then rn of the remainder -- parts = 2 (hi/lo): |x - h - l| <=
  * 2^-16 |x|, about 1e-5 relative error on C, ABOVE the 1e-6 of the TF32
  * form; parts = 3 (hi/mid/lo): <= 2^-24 |x|.  One MMA per 16 rows forms all
- * parts x parts products, FP32 accumulation per 64 rows, FP64 beyond.  A and
+ * parts x parts products, FP32 accumulation per 256 rows, FP64 beyond.  A and
  * B contiguous (lda = m, ldb = k), 16-byte aligned, m and k multiples of 4
  * up to 32 (else TSM_ERROR_UNSUPPORTED).  No counterpart in the reference.
  * Workspace: as tsm_gemm_tn_workspace_size(n, m, k). */

@@ -170,8 +170,8 @@ extern "C" tsm_status tsm_gemm_tn_f32_split_bf16(tsm_stream_t stream, int64_t n,
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return split_fail(e, "cudaGetDevice");
   if (dev < 0 || dev >= 64) return TSM_ERROR_UNSUPPORTED;
-  const void* fn = parts == 2 ? reinterpret_cast<const void*>(&tsm_tn_split_bf16_kernel<2>)
-                              : reinterpret_cast<const void*>(&tsm_tn_split_bf16_kernel<3>);
+  const void* fn = parts == 2 ? reinterpret_cast<const void*>(&tsm_tn_split_bf16_kernel<2, split16::kFlushDefault>)
+                              : reinterpret_cast<const void*>(&tsm_tn_split_bf16_kernel<3, split16::kFlushDefault>);
   const size_t smem = parts == 2 ? split16::Shape<2>::SMEM_BYTES : split16::Shape<3>::SMEM_BYTES;
   {
     std::lock_guard<std::mutex> lk(g_split_mu);

@@ -8,7 +8,7 @@
 //   PARTS = 2 (hi/lo):      |x - h - l|     <= 2^-16 |x|
 //   PARTS = 3 (hi/mid/lo):  |x - h - m - l| <= 2^-24 |x|
 // (each remainder is exact in FP32).  One MMA per 16 rows computes all
-// PARTS x PARTS part products at once, accumulated in FP32 over 128 rows:
+// PARTS x PARTS part products at once, accumulated in FP32 over 256 rows:
 //   D (M = 128, N = 32 PARTS) = [A_0; A_1; ...]  x  [B_0 | B_1 | ...]^T
 // over K = 16 rows: D row 32 p + i is A's part p of column i, D column
 // 32 q + j is B's part q of column j.  The sum over (p, q) of those blocks is
@@ -34,7 +34,7 @@
 //   warps 1, 14, 15  MMA issuers: chunk it goes to issuer it mod 3, which
 //                owns operand stages it mod 6 and TMEM accumulator it mod 3
 //                (issuing from one thread was the bottleneck of the TF32 form)
-//                and accumulates kFlush = 2 of its chunks before a drain
+//                and accumulates kFlush = 4 of its chunks before a drain
 //   warps 10-13  epilogue: warp w reads TMEM lanes 32 w .. +31, i.e. A's part
 //                w (w < PARTS): all PARTS column blocks of 16 columns, one
 //                wait, their FP32 sum (smallest part first) into FP64.  A
@@ -62,7 +62,11 @@ constexpr int kRows = 64;                      // rows per chunk: 4 MMAs of K = 
 constexpr int kIssuers = 3;
 constexpr int kOpStages = 2 * kIssuers;        // two operand stages per issuer: converters run a round ahead
 static_assert(kOpStages % kIssuers == 0, "an operand stage belongs to one issuer");
-constexpr int kFlush = 2;                      // an issuer's chunks per accumulator drain (128 rows)
+// An issuer's chunks per accumulator drain (256 rows).  Against drains every
+// 2 chunks, on one B200 at n = 2^25, 32 x 32 (300-call loops): hi/mid/lo
+// 2.01 vs 2.06 ms (normwise error 1.8e-7 vs 9.7e-8), hi/lo 1.75 vs 1.80 ms
+// (3.0e-6 either way, the split's own error); every 8 chunks gains ~1 % more.
+constexpr int kFlushDefault = 4;
 constexpr int kRawTile = kRows * 32 * 4;       // one operand: 64 rows x 32 floats (8 KB)
 constexpr int kRawStageBytes = 2 * kRawTile;   // A, B
 constexpr int kConvWarps = 8;
@@ -104,11 +108,14 @@ __device__ __forceinline__ float bf16_hi_f32(uint32_t v) { return __uint_as_floa
 
 }  // namespace split16
 
-template <int PARTS>
+// FLUSH: an issuer's chunks accumulated in its TMEM accumulator before a
+// drain (FP32 accumulation over FLUSH * 64 rows).
+template <int PARTS, int FLUSH>
 __global__ void __launch_bounds__(split16::kThreads, 1)
     tsm_tn_split_bf16_kernel(const __grid_constant__ SplitTmaArgs args) {
   using namespace split16;
   using S = Shape<PARTS>;
+  constexpr int kFlush = FLUSH;
   const SplitArgs& p = args.p;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((1024u - (dev::smem_u32(smem_raw) & 1023u)) & 1023u);
