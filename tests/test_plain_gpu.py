@@ -282,3 +282,34 @@ def test_side_stream_with_fresh_workspace_cache(gpu, oracle_mod, monkeypatch):
         monkeypatch.setattr(api, "_workspaces", {})
     torch.cuda.synchronize()
     del busy
+
+
+@pytest.mark.parametrize("m,k", [(8, 8), (16, 16), (64, 64), (3, 5), (1, 64), (32, 4)])
+def test_launch_with_cta_caps(gpu, oracle_mod, m, k):
+    """tsm_gemm_tn_f64_launch caps the grid (the generated drop-in kernels
+    pass the reference's stride / local_size work-groups): every kernel
+    family deals its rows over any grid of 1 CTA or more and gives the same
+    product within the oracle's bounds; a cap above the variant's own grid
+    changes nothing."""
+    from tsm_benchmark_b200 import _capi, default_variant
+    lib = _capi.load()
+    sh = int(torch.cuda.current_stream(gpu).cuda_stream)
+    for n in (777, 100003):
+        A, B = oracle_mod.operands(n, m, k, seed=310 + n + m * k)
+        dA, dB = to_dev(A, gpu), to_dev(B, gpu)
+        need = lib.tsm_gemm_tn_workspace_size(n, m, k)
+        ws = torch.zeros(need, dtype=torch.uint8, device=gpu)
+        ref = oracle_mod.naive(A, B)
+        full = None
+        for cap in (1, 2, 7, 37, 0, 1 << 20):
+            C = torch.full((m, k), float("nan"), dtype=torch.float64, device=gpu)
+            st = lib.tsm_gemm_tn_f64_launch(sh, n, m, k, dA.data_ptr(), m, dB.data_ptr(), k, C.data_ptr(), k, 0,
+                                            ws.data_ptr(), need, -1, cap)
+            assert st == 0, _capi.STATUS[st]
+            torch.cuda.synchronize()
+            assert_parity(oracle_mod, A, B, C, ref, what=f"cap {cap}, n={n} {m}x{k}")
+            if cap == 0:
+                full = C.clone()
+            if cap == 1 << 20:  # above the variant's grid: the same launch as no cap
+                assert torch.equal(C, full)
+        assert default_variant(dA, dB) >= 0
