@@ -605,9 +605,19 @@ def main() -> int:
             t = torch.tensor([ms], dtype=torch.float64, device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
+        # The bound of the end-to-end step: the host-to-device link, measured
+        # here as one pinned copy of A alone (several streams measured the same).
+        l0 = torch.cuda.Event(enable_timing=True)
+        l1 = torch.cuda.Event(enable_timing=True)
+        l0.record(stream)
+        A.copy_(Ah, non_blocking=True)
+        l1.record(stream)
+        torch.cuda.synchronize()
+        link = Ah.numel() * 8 / (l0.elapsed_time(l1) * 1e-3) / 1e9
+        h2d = (Ah.numel() * 8 + Bh.numel() * 8) * world
         e2e = {"value": bytes_step * world / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms,
-               "h2d_bytes_per_step": (Ah.numel() * 8 + Bh.numel() * 8) * world,
-               "d2h_bytes_per_step": Ch.numel() * 8 * world}
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": Ch.numel() * 8 * world,
+               "h2d_link_GB/s": round(link, 2), "frac_of_h2d_link": round(h2d / world / (ms * 1e-3) / 1e9 / link, 4)}
         del Ah, Bh
 
     # ---------------- the precision, batching and differentiation forms
@@ -651,7 +661,8 @@ def summary(line: dict) -> str:
            f"{line['roofline']['achieved']:.1f} GB/s = {line['roofline']['frac']:.3f} of {line['roofline']['peak']} "
            f"({line['roofline']['peak_source']})"]
     if line.get("e2e"):
-        out.append(f"e2e {line['e2e']['value']:.2f} GB/s")
+        out.append(f"e2e {line['e2e']['value']:.2f} GB/s ({line['e2e']['frac_of_h2d_link']:.3f} of the "
+                   f"{line['e2e']['h2d_link_GB/s']} GB/s host-to-device link)")
     for r in line.get("by_width") or []:
         out.append(f"  n=2^{r['n'].bit_length() - 1} {r['m']}x{r['k']}: {r['GB/s']} GB/s, {r['GFLOP/s']} GFLOP/s, "
                    f"{r['bound']} {r['frac_roof']}, {r['variant']}")
