@@ -136,6 +136,14 @@ def test_c_abi_rejects_bad_arguments_before_any_cuda_call():
     assert lib.tsm_gemm_tn_batched_f64(None, None) == INVALID
     assert lib.tsm_gemm_tn_batched_f64(None, ctypes.byref(_capi.BatchedPlan())) == INVALID
     assert lib.tsm_batched_plan_init_f64(None, 1, None, P, 1 << 20, None) == INVALID
+    # per-class paths: -1 (tuned), 0 (tensor cores), 1 (SIMT); others refused before any CUDA call
+    plan = _capi.BatchedPlan()
+    probs = (_capi.BatchedProblem * 1)()
+    for bad in (2, -2, 7):
+        paths = (ctypes.c_int * 16)(*([-1] * 16))
+        paths[10] = bad
+        assert lib.tsm_batched_plan_init_paths_f64(None, 1, probs, paths, P, 1 << 20, ctypes.byref(plan)) == INVALID
+    assert lib.tsm_batched_plan_init_paths_f64(None, 0, probs, None, P, 1 << 20, ctypes.byref(plan)) == INVALID
     # self-test and fill: workspace and count checks
     assert lib.tsm_selftest_wait_timeout(None, None, 0, 1000) == WORKSPACE
     assert lib.tsm_fill_uniform_f64(None, P, -1, 1, 0) == INVALID

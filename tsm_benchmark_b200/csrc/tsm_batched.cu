@@ -217,6 +217,10 @@ tsm_status tsm_batched_plan_init_paths_f64(tsm_stream_t stream, int count, const
                                            const int* class_paths, void* device_buffer, size_t device_bytes,
                                            tsm_batched_plan* plan) {
   if (plan == nullptr || device_buffer == nullptr || !aligned16(device_buffer)) return TSM_ERROR_INVALID_VALUE;
+  if (count < 1 || problems == nullptr) return TSM_ERROR_INVALID_VALUE;
+  if (class_paths != nullptr)  // checked before any CUDA call
+    for (int c = 0; c < 16; ++c)
+      if (class_paths[c] < -1 || class_paths[c] > batched::kPathSimt) return TSM_ERROR_INVALID_VALUE;
   int sms = 0;
   tsm_status st = device_sms(&sms);
   if (st != TSM_SUCCESS) return st;
