@@ -542,6 +542,11 @@ def main() -> int:
         for n, m, k in SWEEP:
             a, b = views(n, m, k)
             c = torch.zeros((m, k), dtype=torch.float64, device=dev)
+            # One second at rest before each shape: every shape starts from the
+            # same power state, as the best-of-5 DGEMM roof does (the FP64-bound
+            # 64 x 64 otherwise inherits the clock the shapes before it left).
+            torch.cuda.synchronize()
+            time.sleep(1.0)
             for _ in range(3):
                 call(a, b, c, n, m, k)
             e0 = torch.cuda.Event(enable_timing=True)
