@@ -34,6 +34,8 @@ def _on_stream(device: torch.device, stream):
     if isinstance(stream, torch.cuda.Stream):
         return torch.cuda.stream(stream)
     if torch.cuda.is_available():
+        if int(stream) == 0:  # the legacy default stream, torch's default stream
+            return torch.cuda.stream(torch.cuda.default_stream(device))
         return torch.cuda.stream(torch.cuda.ExternalStream(int(stream), device=device))
     return contextlib.nullcontext()  # no device: only fake allocators reach here
 
