@@ -87,3 +87,16 @@ def test_compat_templates_match_reference_outputs(gpu, oracle_mod):
         assert nw["err"] <= nw["bound"], (name, nw)
         if name in g:  # the reference kernel of the same name, run on the host
             assert oracle_mod.check(g[name], got[name], 1e-6, 1e-10) == -1, name
+
+
+def test_main_codegen_with_generated_odd_widths(gpu):
+    """main_codegen.cc against a header generated for widths that are not
+    powers of two, --M 12 24 48 --tile-sizes 3 4 6 (capacity kernels,
+    tiles with no compiled match, the 48-wide tensor-core kernel): every one
+    of the 9 (M, TM) pairs x 4 kernels PASSes."""
+    out = run("main_codegen_odd_dropin")
+    rows = re.findall(r"^\s*(M(\d+)_T(\d+)_(\w+))\s+(PASS|FAIL)", out, flags=re.M)
+    pairs = {(int(m), int(t)) for _, m, t, _, _ in rows}
+    assert pairs == {(m, t) for m in (12, 24, 48) for t in (3, 4, 6) if m % t == 0}, pairs
+    assert len(rows) == 4 * len(pairs)
+    assert all(s == "PASS" for *_, s in rows), [r for r in rows if r[-1] != "PASS"]
