@@ -55,13 +55,14 @@ struct SplitTmaArgs {
 
 namespace split2 {
 
-// Constants of the kernel for chunks of ROWS rows (ROWS / 8 MMAs of K = 8).
-template <int ROWS>
+// Constants of the kernel for chunks of ROWS rows (ROWS / 8 MMAs of K = 8)
+// and ISSUERS MMA-issuing warps.
+template <int ROWS, int ISSUERS = 3>
 struct Cfg {
   static constexpr int kRows = ROWS;
   // kIssuers warps issue the MMAs (chunk it goes to issuer it % kIssuers);
   // each owns one lo stage and one TMEM accumulator.
-  static constexpr int kIssuers = 3;
+  static constexpr int kIssuers = ISSUERS;
   static constexpr int kTileBytes = kRows * 128;      // one operand part: 32 floats x kRows rows
   static constexpr int kStageBytes = 2 * kTileBytes;  // A part, B part
   static constexpr int kLoStages = kIssuers;
@@ -101,10 +102,10 @@ __device__ __forceinline__ uint32_t lo_part(uint32_t xb) {
 
 // DRAIN: chunks of one issuer accumulated in its TMEM accumulator before the
 // epilogue drains it (FP32 accumulation over DRAIN * ROWS rows).
-template <int ROWS, int DRAIN>
-__global__ void __launch_bounds__(split2::Cfg<ROWS>::kThreads, 1)
+template <int ROWS, int DRAIN, int ISSUERS = 3>
+__global__ void __launch_bounds__(split2::Cfg<ROWS, ISSUERS>::kThreads, 1)
     tsm_tn_split_tf32_tma_kernel(const __grid_constant__ SplitTmaArgs args) {
-  using S = split2::Cfg<ROWS>;
+  using S = split2::Cfg<ROWS, ISSUERS>;
   static_assert(DRAIN >= 1, "at least one chunk per drain");
   using split2::kIdesc;
   using split2::lo_part;
