@@ -341,7 +341,7 @@ def forms(dev) -> dict:
     # --- Gram C = A^T A (A streamed once, upper triangle) vs the two-operand
     #     call on a copy of A
     rows = []
-    for gm, gn in ((8, 1 << 26), (32, 1 << 26), (64, 1 << 23)):
+    for gm, gn in ((8, 1 << 26), (16, 1 << 26), (32, 1 << 26), (64, 1 << 23)):
         A = torch.empty((gn, gm), dtype=torch.float64, device=dev)
         tsm.fill_uniform(A, 77, 0)
         A2 = A.clone()

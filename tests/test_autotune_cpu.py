@@ -98,3 +98,46 @@ def test_batched_paths_reach_the_generated_table(tmp_path):
     files = codegen.render(codegen.default_variants(), [], batched_paths=codegen.load_tuned_batched(str(path)))
     idx = files["variants_index.cu"]
     assert '"16 16 1",' in idx and '"32 32 0",' in idx and "kTunedBatchedPathCount = 2;" in idx
+
+
+def test_gram_choices_reach_the_generated_table(tmp_path):
+    """tuned.json's gram_choices become the library's Gram table (kTunedGram
+    in csrc/generated/variants_index.cu); a name that is not a Gram variant
+    is rejected."""
+    import json
+
+    import pytest
+
+    from tsm_benchmark_b200 import codegen
+    doc = {"choices": [], "gram_choices": [{"w": 16, "nmin": 8388608, "variant": "dmma_16x16_gram_w8_s2_r768"},
+                                           {"w": 16, "nmin": 0, "variant": "dmma_16x16_gram_w8_s4_r256"}]}
+    path = tmp_path / "tuned.json"
+    path.write_text(json.dumps(doc))
+    gram = codegen.load_tuned_gram(str(path))
+    assert gram == [(16, 0, "dmma_16x16_gram_w8_s4_r256"), (16, 8388608, "dmma_16x16_gram_w8_s2_r768")]
+    files = codegen.render(codegen.default_variants(), [], batched_paths=[], gram=gram)
+    idx = files["variants_index.cu"]
+    assert '"16 8388608 dmma_16x16_gram_w8_s2_r768",' in idx and "kTunedGramCount = 2;" in idx
+    with pytest.raises(ValueError, match="not a Gram variant"):
+        codegen.render(codegen.default_variants(), [], batched_paths=[], gram=[(16, 0, "dmma_16x16_t16x16_w8_s2_r384")])
+
+
+def test_gram_candidates():
+    """Gram candidates: Gram variants only, exact ones of the width, capacity
+    ones up to twice the smallest capacity; every width of the tuner has one."""
+    from tsm_benchmark_b200.autotune import GRAM_WIDTHS, gram_candidates
+    vs = [
+        {"name": "g16a", "gram": True, "dtype": "f64", "exact": True, "wa": 16, "wb": 16},
+        {"name": "g16b", "gram": True, "dtype": "f64", "exact": True, "wa": 16, "wb": 16},
+        {"name": "p16", "gram": False, "dtype": "f64", "exact": True, "wa": 16, "wb": 16},
+        {"name": "c8", "gram": True, "dtype": "f64", "exact": False, "wa": 8, "wb": 8},
+        {"name": "c32", "gram": True, "dtype": "f64", "exact": False, "wa": 32, "wb": 32},
+        {"name": "f16", "gram": True, "dtype": "f32", "exact": True, "wa": 16, "wb": 16},
+    ]
+    assert [v["name"] for v in gram_candidates(vs, 16)] == ["g16a", "g16b", "c32"]
+    assert [v["name"] for v in gram_candidates(vs, 5)] == ["c8"]
+    from tsm_benchmark_b200 import codegen
+    real = [{"name": v.name, "gram": getattr(v, "gram", False), "dtype": v.dtype, "exact": v.exact,
+             "wa": v.wa, "wb": v.wb} for v in codegen.default_variants()]
+    for w in GRAM_WIDTHS:
+        assert gram_candidates(real, w), w

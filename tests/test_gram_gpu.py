@@ -20,6 +20,20 @@ def test_gram_parity_and_symmetry(gpu, oracle_mod, m):
         assert torch.equal(C, C.T), (m, n)
 
 
+def test_every_gram_variant(gpu, oracle_mod):
+    """Every compiled Gram variant (each ring shape, chunks of one or several
+    tensor boxes) on row counts around its chunk and box edges."""
+    from tsm_benchmark_b200 import tsmttsm, variants
+    for v in (v for v in variants() if v["gram"] and v["dtype"] == "f64"):
+        m = v["wa"]
+        for n in (1, 5, v["rows"] // 2 + 1, v["rows"] - 1, v["rows"] + 3, 3 * v["rows"] + 11, 40013):
+            A, _ = oracle_mod.operands(n, m, m, 70 + m + n % 31)
+            dA = to_dev(A, gpu)
+            C = tsmttsm(dA, dA, variant=v["index"])
+            assert_parity(oracle_mod, A, A, C, what=f"{v['name']} n={n}")
+            assert torch.equal(C, C.T), (v["name"], n)
+
+
 def test_gram_variant_is_chosen_for_same_operand(gpu, oracle_mod):
     from tsm_benchmark_b200 import default_variant, tsmttsm, variants
     vs = variants()

@@ -4,6 +4,7 @@
     python -m tsm_benchmark_b200.autotune [--shapes sweep|batched|all] [--out tuned.json]
     python -m tsm_benchmark_b200.autotune --shapes batched-paths   (the batched kernel's path per class)
     python -m tsm_benchmark_b200.autotune --pairs 8x8 --merge        (re-tune one shape, keep the rest)
+    python -m tsm_benchmark_b200.autotune --shapes gram              (the Gram variant per width, C = A^T A)
 
 For every width pair and row bucket it times each applicable variant of the
 table (CUDA events, warm-up then repeated launches, inputs larger than L2
@@ -33,6 +34,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "tuned.json")
 
 SWEEP_PAIRS = [(1, 1), (2, 2), (4, 4), (8, 8), (16, 16), (32, 32), (64, 64), (4, 32), (32, 4), (1, 64)]
+GRAM_WIDTHS = [1, 2, 4, 8, 16, 32, 48, 64]
+# Sections of tuned.json that one mode writes and the others keep.
+KEPT_SECTIONS = ("batched_paths", "gram_choices", "gram_timings")
 BATCHED_PAIRS = [(a, b) for a in (4, 8, 16, 32) for b in (4, 8, 16, 32)]
 # (nmin, n to time at): the largest nmin <= n selects the entry at run time.
 BUCKETS = [(0, 1 << 15), (1 << 18, 1 << 20), (1 << 23, 1 << 26)]
@@ -62,6 +66,15 @@ def candidates(variants: list[dict], m: int, k: int, dtype: str = "f64") -> list
         elif m <= v["wa"] <= 2 * cm and k <= v["wb"] <= 2 * ck:
             out.append(v)
     return out
+
+
+def gram_candidates(variants: list[dict], w: int, dtype: str = "f64") -> list[dict]:
+    """Gram variants (C = A^T A, A streamed once) of `dtype` that take width
+    `w`: the exact ones of that width, and capacity ones no more than twice
+    the smallest capacity."""
+    cw = _cap(w)
+    return [v for v in variants if v.get("gram") and v["dtype"] == dtype and
+            (v["wa"] == w if v["exact"] else w <= v["wa"] <= 2 * cw)]
 
 
 def refinement_set(row: dict, within: float = 1.05, top_n: int = 3) -> list[str]:
@@ -107,6 +120,26 @@ def time_variant(call, reps: int, warmup: int = 3) -> float:
     return e0.elapsed_time(e1) / reps
 
 
+def refine(row: dict, make_call, nbytes: int, reps_time_ms: float, rounds: int):
+    """The top candidates of `row` (within 5 % of the fastest single timing),
+    timed in interleaved rounds (A B C A B C ...) and decided by the median --
+    single timings of near-equal kernels differ by a few percent from run to
+    run, more than the kernels do.  Records each one's median in `row` and
+    returns (name, ms, GB/s) of the winner, or None with fewer than two."""
+    top = refinement_set(row)
+    if len(top) < 2:
+        return None
+    reps = max(3, min(100, int(reps_time_ms / 3 / max(row[top[0]]["ms"], 1e-3))))
+    samples = {name: [] for name in top}
+    for _ in range(rounds):
+        for name in top:
+            samples[name].append(time_variant(make_call(name), reps, warmup=1))
+    win, med = median_winner(samples)
+    for name in top:
+        row[name]["median_ms_interleaved"] = round(med[name], 5)
+    return (win, med[win], nbytes / (med[win] * 1e-3) / 1e9)
+
+
 def tune(pairs, buckets=BUCKETS, reps_time_ms: float = 150.0, verbose: bool = True, rounds: int = 5) -> dict:
     import torch
 
@@ -144,23 +177,9 @@ def tune(pairs, buckets=BUCKETS, reps_time_ms: float = 150.0, verbose: bool = Tr
                 row[v["name"]] = {"ms": round(ms, 5), "GB/s": round(gbs, 1), "ok": ok}
                 if ok and (best is None or ms < best[1]):
                     best = (v["name"], ms, gbs)
-            # Refinement: the top candidates within 5 % of the best, timed in
-            # interleaved rounds (A B C A B C ...), decided by the median --
-            # single timings of near-equal kernels differ by a few percent
-            # from run to run, more than the kernels do.
-            top = refinement_set(row)
-            if len(top) > 1:
-                idx = {v["name"]: v["index"] for v in vs}
-                reps = max(3, min(100, int(reps_time_ms / 3 / max(row[top[0]]["ms"], 1e-3))))
-                samples = {name: [] for name in top}
-                for _ in range(rounds):
-                    for name in top:
-                        call = lambda: tsmttsm(A, B, C, variant=idx[name])  # noqa: E731
-                        samples[name].append(time_variant(call, reps, warmup=1))
-                win, med = median_winner(samples)
-                for name in top:
-                    row[name]["median_ms_interleaved"] = round(med[name], 5)
-                best = (win, med[win], 8 * n * (m + k) / (med[win] * 1e-3) / 1e9)
+            idx = {v["name"]: v["index"] for v in vs}
+            best = refine(row, lambda name: (lambda: tsmttsm(A, B, C, variant=idx[name])), 8 * n * (m + k),
+                          reps_time_ms, rounds) or best
             timings[f"{m}x{k}@{n}"] = row
             if best:
                 choices.append({"m": m, "k": k, "nmin": nmin, "n_timed": n, "variant": best[0],
@@ -172,6 +191,57 @@ def tune(pairs, buckets=BUCKETS, reps_time_ms: float = 150.0, verbose: bool = Tr
             torch.cuda.empty_cache()
     return {"device": torch.cuda.get_device_name(dev), "dtype": "f64", "when": time.strftime("%Y-%m-%d %H:%M:%S"),
             "choices": choices, "timings": timings}
+
+
+def tune_gram(widths=GRAM_WIDTHS, buckets=BUCKETS, reps_time_ms: float = 150.0, verbose: bool = True,
+              rounds: int = 5) -> dict:
+    """For each width and row bucket, every Gram variant that takes the width
+    (C = A^T A through tsmttsm(A, A)), timed like the plain variants; each
+    result must be exactly symmetric and within the normwise bound of the
+    first one's.  Returns {"gram_choices": [...], "gram_timings": {...}}."""
+    import torch
+
+    from . import variants as list_variants
+    from .api import fill_uniform, tsmttsm
+
+    dev = torch.device("cuda", 0)
+    vs = list_variants()
+    idx = {v["name"]: v["index"] for v in vs}
+    choices, timings = [], {}
+    for w in widths:
+        for nmin, n in buckets:
+            while n > 1 << 12 and 8 * n * w > MAX_BYTES:
+                n //= 2
+            A = torch.empty((n, w), dtype=torch.float64, device=dev)
+            fill_uniform(A, 3, 0)
+            bound = 8 * math.sqrt(n) * 2.0**-53 * float(torch.linalg.norm(A)) ** 2
+            C = torch.empty((w, w), dtype=torch.float64, device=dev)
+            ref, best, row = None, None, {}
+            for v in gram_candidates(vs, w):
+                call = lambda: tsmttsm(A, A, C, variant=v["index"])  # noqa: E731
+                t0 = time_variant(call, 1, warmup=1)
+                reps = max(3, min(200, int(reps_time_ms / max(t0, 1e-3))))
+                ms = time_variant(call, reps)
+                got = C.clone()
+                if ref is None:
+                    ref = got
+                ok = bool(torch.equal(got, got.T)) and float(torch.linalg.norm(got - ref)) <= 2 * bound
+                gbs = 8 * n * w / (ms * 1e-3) / 1e9
+                row[v["name"]] = {"ms": round(ms, 5), "GB/s": round(gbs, 1), "ok": ok}
+                if ok and (best is None or ms < best[1]):
+                    best = (v["name"], ms, gbs)
+            best = refine(row, lambda name: (lambda: tsmttsm(A, A, C, variant=idx[name])), 8 * n * w,
+                          reps_time_ms, rounds) or best
+            timings[f"gram{w}@{n}"] = row
+            if best:
+                choices.append({"w": w, "nmin": nmin, "n_timed": n, "variant": best[0],
+                                "ms": round(best[1], 5), "GB/s": round(best[2], 1)})
+                if verbose:
+                    print(f"gram {w:>2} n={n:>9}: {best[0]:<40} {best[2]:8.1f} GB/s ({len(row)} candidates)",
+                          flush=True)
+            del A
+            torch.cuda.empty_cache()
+    return {"gram_choices": choices, "gram_timings": timings}
 
 
 # Width classes of the batched kernel with two compiled consumer paths.
@@ -229,25 +299,30 @@ def tune_batched_paths(count: int = 96, rounds: int = 5, reps: int = 10, seed: i
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--shapes", choices=["sweep", "batched", "batched-paths", "all"], default="all",
-                    help="batched-paths: the batched kernel's consumer path per tensor-core class "
-                         "(kept beside the other choices of --out)")
+    ap.add_argument("--shapes", choices=["sweep", "batched", "batched-paths", "gram", "all"], default="all",
+                    help="batched-paths: the batched kernel's consumer path per tensor-core class; "
+                         "gram: the Gram variant per width (each kept beside the other choices of --out)")
     ap.add_argument("--out", default=DEFAULT_OUT)
     ap.add_argument("--budget-ms", type=float, default=150.0, help="timed milliseconds per candidate")
     ap.add_argument("--pairs", default=None, help="only these width pairs, e.g. 8x8,16x16 (overrides --shapes)")
     ap.add_argument("--merge", action="store_true",
                     help="keep the other pairs' choices and timings of an existing --out file")
     args = ap.parse_args(argv)
-    if args.shapes == "batched-paths":
+    if args.shapes in ("batched-paths", "gram"):
         old = {}
         if os.path.exists(args.out):
             with open(args.out) as f:
                 old = json.load(f)
-        old["batched_paths"] = tune_batched_paths()
+        if args.shapes == "gram":
+            old.update(tune_gram(reps_time_ms=args.budget_ms))
+            what = f"{len(old['gram_choices'])} Gram choices"
+        else:
+            old["batched_paths"] = tune_batched_paths()
+            what = f"{len(old['batched_paths'])} batched paths"
         with open(args.out, "w") as f:
             json.dump(old, f, indent=1)
             f.write("\n")
-        print(f"wrote {args.out}: {len(old['batched_paths'])} batched paths")
+        print(f"wrote {args.out}: {what}")
         return 0
     pairs = {"sweep": SWEEP_PAIRS, "batched": BATCHED_PAIRS,
              "all": sorted(set(SWEEP_PAIRS + BATCHED_PAIRS))}[args.shapes]
@@ -257,11 +332,12 @@ def main(argv=None) -> int:
     if args.merge and os.path.exists(args.out):
         with open(args.out) as f:
             res = merge_results(json.load(f), res, pairs)
-    if os.path.exists(args.out) and "batched_paths" not in res:
+    if os.path.exists(args.out):
         with open(args.out) as f:
-            kept = json.load(f).get("batched_paths")
-        if kept:
-            res["batched_paths"] = kept
+            old = json.load(f)
+        for key in KEPT_SECTIONS:
+            if key not in res and key in old:
+                res[key] = old[key]
     with open(args.out, "w") as f:
         json.dump(res, f, indent=1)
         f.write("\n")

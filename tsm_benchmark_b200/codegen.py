@@ -277,8 +277,9 @@ class DmmaVariant:
             errs.append("consumer warps must cover whole regions")
         if v.cw > 12:
             errs.append("more than 12 consumer warps (register cap)")
-        if v.rows % 8 or v.rows > 256:
-            errs.append("chunk rows: multiple of 8, at most 256")
+        boxes = -(-v.rows // 256)  # tensor boxes of at most 256 rows per 16-column block
+        if v.rows <= 0 or v.rows % 8 or v.rows > 1024 or v.rows % boxes or (v.rows // boxes) % 8:
+            errs.append("chunk rows: equal boxes of whole 8-row groups, at most 256 rows each")
         if (v.rows // 4) % (v.cw // v.regions):
             errs.append("chunk k-steps must split evenly over the row slots")
         if v.dtype != "f64":
@@ -406,6 +407,12 @@ def default_variants() -> list:
     # FP64 tensor-core kernels with other ring shapes (autotuner candidates)
     for wa, rows, stages in ((16, 192, 4), (16, 128, 6), (32, 96, 4), (32, 192, 2), (32, 64, 6)):
         out.append(DmmaVariant(wa, wa, rows=rows, stages=stages))
+    # Longer chunks for 16 x 16 (two tensor boxes per block and chunk): 2 x 96 KB
+    # and 3 x 72 KB; the Gram kernel of width 16 with 2 x 96 KB and 3 x 64 KB.
+    for rows, stages in ((384, 2), (288, 3)):
+        out.append(DmmaVariant(16, 16, rows=rows, stages=stages))
+    for rows, stages in ((768, 2), (512, 3)):
+        out.append(DmmaVariant(16, 16, rows=rows, stages=stages, gram=True))
     return out
 
 
@@ -434,6 +441,15 @@ def load_tuned_batched(path: str = TUNED_JSON) -> list[tuple[int, int, int]]:
     return sorted((int(e["m"]), int(e["k"]), BATCHED_PATHS[e["path"]]) for e in doc.get("batched_paths", []))
 
 
+def load_tuned_gram(path: str = TUNED_JSON) -> list[tuple[int, int, str]]:
+    """Tuned Gram variants (C = A^T A): list of (width, nmin, variant name)."""
+    if not os.path.exists(path):
+        return []
+    with open(path) as f:
+        doc = json.load(f)
+    return sorted((int(e["w"]), int(e.get("nmin", 0)), str(e["variant"])) for e in doc.get("gram_choices", []))
+
+
 def load_tuned(path: str = TUNED_JSON) -> list[tuple[int, int, int, str]]:
     """Tuned defaults: list of (m, k, nmin, variant name)."""
     if not os.path.exists(path):
@@ -450,15 +466,22 @@ HEADER = ("// Generated by tsm_benchmark_b200/codegen.py -- do not edit.\n"
           "// Regenerate with: python -m tsm_benchmark_b200.codegen\n")
 
 
-def render(vs: list, tuned: list, parts: int = 8, batched_paths: list | None = None) -> dict[str, str]:
+def render(vs: list, tuned: list, parts: int = 8, batched_paths: list | None = None,
+           gram: list | None = None) -> dict[str, str]:
     """Returns {file name: contents} for csrc/generated/."""
     if batched_paths is None:
         batched_paths = load_tuned_batched()
+    if gram is None:
+        gram = load_tuned_gram()
     check_variants(vs)
     known = {v.name for v in vs}
     for m, k, nmin, name in tuned:
         if name not in known:
             raise ValueError(f"tuned choice {name} for ({m},{k}) is not a variant")
+    grams = {v.name for v in vs if getattr(v, "gram", False)}
+    for w, nmin, name in gram:
+        if name not in grams:
+            raise ValueError(f"tuned Gram choice {name} for width {w} is not a Gram variant")
     files: dict[str, str] = {}
     chunks = [vs[i::parts] for i in range(parts)]
     # Keep table order global: part i holds rows i, i+parts, ...; the index
@@ -504,6 +527,15 @@ def render(vs: list, tuned: list, parts: int = 8, batched_paths: list | None = N
     idx.append("    nullptr};")
     idx.append("extern const int kTunedBatchedPathCount;")
     idx.append(f"const int kTunedBatchedPathCount = {len(batched_paths)};")
+    idx.append("")
+    idx.append("// Tuned Gram variants (C = A^T A): \"w nmin variant\" (largest nmin <= n wins).")
+    idx.append("extern const char* const kTunedGram[];")
+    idx.append("const char* const kTunedGram[] = {")
+    for w, nmin, name in gram:
+        idx.append(f'    "{w} {nmin} {name}",')
+    idx.append("    nullptr};")
+    idx.append("extern const int kTunedGramCount;")
+    idx.append(f"const int kTunedGramCount = {len(gram)};")
     idx.append("")
     idx.append("}  // namespace tsm")
     files["variants_index.cu"] = "\n".join(idx) + "\n"
@@ -777,7 +809,8 @@ def main(argv=None) -> int:
     if not os.path.exists(COMPAT_HEADER) or open(COMPAT_HEADER).read() != compat:
         with open(COMPAT_HEADER, "w") as f:
             f.write(compat)
-    print(f"wrote {len(files)} files, {len(vs)} variants, {len(load_tuned())} tuned choices to {args.out}")
+    print(f"wrote {len(files)} files, {len(vs)} variants, {len(load_tuned())} tuned choices, "
+          f"{len(load_tuned_gram())} tuned Gram choices to {args.out}")
     return 0
 
 

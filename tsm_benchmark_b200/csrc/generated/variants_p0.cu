@@ -51,8 +51,9 @@ const Variant kGenPart0[] = {
     TSM_DIRECT_VARIANT("directf32_64x16_t8x8_th256_cap", float, 64, 16, 8, 8, 256, false),
     TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s2_r6144_u1_gram", double, 2, 2, 2, 2, 8, 2, 6144, 1, true, true),
     TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r2048_u1_gram", double, 2, 2, 2, 2, 8, 6, 2048, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s2_r384", 16, 16, 2, 2, 8, 2, 384),
 };
 extern const int kGenPart0Count;
-const int kGenPart0Count = 44;
+const int kGenPart0Count = 45;
 
 }  // namespace tsm

@@ -51,8 +51,9 @@ const Variant kGenPart1[] = {
     TSM_DIRECT_VARIANT("directf32_64x32_t8x8_th256_cap", float, 64, 32, 8, 8, 256, false),
     TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s2_r3072_u1_gram", double, 4, 4, 4, 4, 8, 2, 3072, 1, true, true),
     TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r1024_u1_gram", double, 4, 4, 4, 4, 8, 6, 1024, 1, true, true),
+    TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s3_r288", 16, 16, 2, 2, 8, 3, 288),
 };
 extern const int kGenPart1Count;
-const int kGenPart1Count = 44;
+const int kGenPart1Count = 45;
 
 }  // namespace tsm

@@ -138,6 +138,8 @@ tsm_status encode_operand_map(CUtensorMap* map, const double* base, int64_t rows
 
 extern const char* const kTunedDefaults[];  // "m k nmin name", null-terminated
 extern const int kTunedDefaultCount;
+extern const char* const kTunedGram[];  // "w nmin name": Gram variants, null-terminated
+extern const int kTunedGramCount;
 
 namespace {
 
@@ -150,10 +152,27 @@ int find_variant(const char* name) {
 
 int default_variant(int dtype, int64_t n, int m, int k, const void* A, int64_t lda, const void* B, int64_t ldb) {
   const auto& vs = variants();
-  // 0. C = A^T A: a Gram variant (A streamed once), in table order.
-  if (is_gram(m, k, A, lda, B, ldb))
+  // 0. C = A^T A: a Gram variant (A streamed once): the tuned entry with the
+  //    largest nmin <= n for width m, else the first in table order.
+  if (is_gram(m, k, A, lda, B, ldb)) {
+    int best = -1;
+    long long best_nmin = -1;
+    for (int i = 0; i < kTunedGramCount; ++i) {
+      int tw = 0;
+      long long nmin = 0;
+      char name[96] = {0};
+      if (std::sscanf(kTunedGram[i], "%d %lld %95s", &tw, &nmin, name) != 3) continue;
+      if (tw != m || nmin > n || nmin < best_nmin) continue;
+      const int idx = find_variant(name);
+      if (idx >= 0 && vs[idx]->gram && applicable(vs[idx], dtype, n, m, k, A, lda, B, ldb)) {
+        best = idx;
+        best_nmin = nmin;
+      }
+    }
+    if (best >= 0) return best;
     for (size_t i = 0; i < vs.size(); ++i)
       if (vs[i]->gram && applicable(vs[i], dtype, n, m, k, A, lda, B, ldb)) return static_cast<int>(i);
+  }
   // 1. The tuning table: the entry with the largest nmin <= n for (m, k).
   int best = -1;
   long long best_nmin = -1;
@@ -237,8 +256,9 @@ tsm_status launch_variant(const Variant* v, const PlainArgs<T>& p, int64_t grid,
       d.p = p;
       d.p.symmetric = is_gram(p.m, p.k, p.A, p.lda, p.B, p.ldb) ? 1 : 0;
       if (p.n > 0) {  // n = 0: no chunks, the maps are never read
-        tsm_status s = encode_operand_map(&d.ta, p.A, p.n, p.m, p.lda, v->rows);
-        if (s == TSM_SUCCESS && !v->gram) s = encode_operand_map(&d.tb, p.B, p.n, p.k, p.ldb, v->rows);
+        const int box_rows = dmma_box_rows(v->rows);
+        tsm_status s = encode_operand_map(&d.ta, p.A, p.n, p.m, p.lda, box_rows);
+        if (s == TSM_SUCCESS && !v->gram) s = encode_operand_map(&d.tb, p.B, p.n, p.k, p.ldb, box_rows);
         if (s != TSM_SUCCESS) return s;
       }
       void* args[] = {&d};

@@ -51,11 +51,23 @@ struct DmmaArgs {
   CUtensorMap tb;  // B: {k columns, n rows}, box {16, RS}, 128-byte swizzle
 };
 
+// A chunk of RS rows is loaded as dmma_boxes(RS) tensor boxes of
+// dmma_box_rows(RS) rows per 16-column block (a box spans at most 256 rows;
+// each box is a whole number of 8-row swizzle groups, 1024-byte aligned, so
+// the block's rows lie in shared memory exactly as one taller box would put
+// them).  The host encodes the tensor maps with the same box height.
+__host__ __device__ constexpr int dmma_boxes(int rs) { return (rs + 255) / 256; }
+__host__ __device__ constexpr int dmma_box_rows(int rs) { return rs / dmma_boxes(rs); }
+__host__ __device__ constexpr bool dmma_rows_ok(int rs) {
+  return rs > 0 && rs % 8 == 0 && rs <= 1024 && rs % dmma_boxes(rs) == 0 && dmma_box_rows(rs) % 8 == 0;
+}
+
 template <int WA, int WB, int MT, int NT, int CW, int STAGES, int RS>
 struct DmmaTn {
   static_assert(WA % 16 == 0 && WB % 16 == 0 && WA <= 64 && WB <= 64, "widths: multiples of 16 up to 64");
-  static_assert(RS % 8 == 0 && RS <= 256, "chunk rows: whole 8-row swizzle groups, TMA box <= 256");
-  static constexpr int MBA = WA / 16, MBB = WB / 16;  // 16-column blocks (TMA boxes) per chunk
+  static_assert(dmma_rows_ok(RS), "chunk rows: equal boxes of whole 8-row swizzle groups, <= 256 rows each");
+  static constexpr int NBOX = dmma_boxes(RS), BOX_ROWS = dmma_box_rows(RS);
+  static constexpr int MBA = WA / 16, MBB = WB / 16;  // 16-column blocks per chunk
   static constexpr int MTA = WA / 8, NTB = WB / 8;    // 8 x 8 tiles of C along m and k
   // MT x NT tiles per warp (region): even (whole 16-column blocks), dividing
   // the widths, at most 16 tiles (32 accumulators per lane).
@@ -66,7 +78,7 @@ struct DmmaTn {
   static_assert(CW % R == 0, "consumer warps must cover whole regions");
   static constexpr int S = CW / R;  // row slots
   static constexpr int KSTEPS = RS / 4;
-  static constexpr int BOX_BYTES = RS * 128;
+  static constexpr int BOX_BYTES = RS * 128;  // one 16-column block of the chunk (NBOX tensor boxes)
   static constexpr int STAGE_BYTES = (MBA + MBB) * BOX_BYTES;  // a multiple of 1024
   static constexpr int THREADS = CW * 32 + 32;
   static constexpr size_t RING_BYTES = size_t(STAGES) * STAGE_BYTES;
@@ -129,11 +141,15 @@ __global__ void __launch_bounds__(DmmaTn<WA, WB, MT, NT, CW, STAGES, RS>::THREAD
           const int y = static_cast<int>(c * RS);
           dev::mbar_arrive_expect_tx(&full[s], K::STAGE_BYTES);
 #pragma unroll
-          for (int b = 0; b < K::MBA; ++b)
-            dev::tma_load_2d(stage + b * K::BOX_BYTES, &args.ta, 16 * b, y, &full[s], policy);
+          for (int q = 0; q < K::NBOX; ++q) {
+            const int off = q * K::BOX_ROWS * 128, yq = y + q * K::BOX_ROWS;
 #pragma unroll
-          for (int b = 0; b < K::MBB; ++b)
-            dev::tma_load_2d(stage + (K::MBA + b) * K::BOX_BYTES, &args.tb, 16 * b, y, &full[s], policy);
+            for (int b = 0; b < K::MBA; ++b)
+              dev::tma_load_2d(stage + b * K::BOX_BYTES + off, &args.ta, 16 * b, yq, &full[s], policy);
+#pragma unroll
+            for (int b = 0; b < K::MBB; ++b)
+              dev::tma_load_2d(stage + (K::MBA + b) * K::BOX_BYTES + off, &args.tb, 16 * b, yq, &full[s], policy);
+          }
         } else {
           *abort = 1;
           atomicOr(p.error, dev::kErrTimeout);
@@ -260,13 +276,14 @@ __host__ __device__ constexpr unsigned gram_block_mask(int W, int r) {
 template <int W, int CW, int STAGES, int RS>
 struct GramDmma {
   static_assert(W % 16 == 0 && W >= 16 && W <= 64, "width: multiple of 16 up to 64");
-  static_assert(RS % 8 == 0 && RS <= 256, "chunk rows: whole 8-row swizzle groups, TMA box <= 256");
+  static_assert(dmma_rows_ok(RS), "chunk rows: equal boxes of whole 8-row swizzle groups, <= 256 rows each");
+  static constexpr int NBOX = dmma_boxes(RS), BOX_ROWS = dmma_box_rows(RS);
   static constexpr int NB = W / 16;
   static constexpr int R = gram_regions(W);
   static_assert(CW % R == 0, "consumer warps must cover whole regions");
   static constexpr int S = CW / R;
   static constexpr int KSTEPS = RS / 4;
-  static constexpr int BOX_BYTES = RS * 128;
+  static constexpr int BOX_BYTES = RS * 128;  // one 16-column block of the chunk (NBOX tensor boxes)
   static constexpr int STAGE_BYTES = NB * BOX_BYTES;
   static constexpr int THREADS = CW * 32 + 32;
   static constexpr size_t RING_BYTES = size_t(STAGES) * STAGE_BYTES;
@@ -398,8 +415,11 @@ __global__ void __launch_bounds__(GramDmma<W, CW, STAGES, RS>::THREADS, 1)
           const int y = static_cast<int>(c * RS);
           dev::mbar_arrive_expect_tx(&full[s], K::STAGE_BYTES);
 #pragma unroll
-          for (int b = 0; b < K::NB; ++b)
-            dev::tma_load_2d(stage + b * K::BOX_BYTES, &args.ta, 16 * b, y, &full[s], policy);
+          for (int q = 0; q < K::NBOX; ++q)
+#pragma unroll
+            for (int b = 0; b < K::NB; ++b)
+              dev::tma_load_2d(stage + b * K::BOX_BYTES + q * K::BOX_ROWS * 128, &args.ta, 16 * b,
+                               y + q * K::BOX_ROWS, &full[s], policy);
         } else {
           *abort = 1;
           atomicOr(p.error, dev::kErrTimeout);
