@@ -356,6 +356,27 @@ def forms(dev) -> dict:
         torch.cuda.empty_cache()
     out["gram"] = rows
 
+    # --- block orthogonalisation B <- B - A (A^T B): C = A^T B, then the TSMM
+    #     (two passes: A and B read twice, B written once).  A's columns are
+    #     scaled to about unit norm, so repeated steps keep B bounded.
+    rows = []
+    for om, on in ((8, 1 << 25), (16, 1 << 24), (32, 1 << 23)):
+        A = torch.empty((on, om), dtype=torch.float64, device=dev)
+        B = torch.empty((on, om), dtype=torch.float64, device=dev)
+        tsm.fill_uniform(A, 78, 0)
+        tsm.fill_uniform(B, 78, 1)
+        A.mul_((3.0 / on) ** 0.5)
+        Co = torch.empty((om, om), dtype=torch.float64, device=dev)
+        ms_o = _time(lambda: tsm.block_orthogonalize(A, B, Co), 10)
+        ms_f = _time(lambda: tsm.tsmttsm(A, B, Co), 10)
+        nbytes = 8 * on * (2 * om + 3 * om)
+        rows.append({"n": on, "m": om, "k": om, "orth_ms": round(ms_o, 4), "tsmttsm_ms": round(ms_f, 4),
+                     "over_tsmttsm": round(ms_o / ms_f, 3), "algorithmic_bytes": nbytes,
+                     "GB/s": round(nbytes / (ms_o * 1e-3) / 1e9, 1), "finite": bool(torch.isfinite(B).all())})
+        del A, B
+        torch.cuda.empty_cache()
+    out["block_orth"] = rows
+
     # --- column-major operands (A^T, B^T stored row-major, through
     #     tsm_gemm_tn_strided_f64) vs the row-major call on the same values
     rows = []
@@ -685,6 +706,12 @@ def summary(line: dict) -> str:
             x = f[key]
             out.append(f"  {key}: fwd {x['fwd_ms']} ms, bwd {x['bwd_ms']} ms ({x['bwd_over_fwd']}x; "
                        f"{x['bwd_over_copy']}x a D2D copy of the same bytes)")
+    for x in f.get("gram") or []:
+        out.append(f"  gram {x['m']} at n={x['n']}: {x['gram_ms']} ms, {x['GB/s_of_A']} GB/s of A, "
+                   f"{x['speedup']}x the two-operand call")
+    for x in f.get("block_orth") or []:
+        out.append(f"  block_orth {x['m']}x{x['k']} at n={x['n']}: {x['orth_ms']} ms, {x['GB/s']} GB/s, "
+                   f"{x['over_tsmttsm']}x one TSMTTSM")
     if line.get("cpu_baseline"):
         c = line["cpu_baseline"]
         out.append(f"cpu baseline ({c['kind']}, {c['cores']} cores): {c['value']:.3f} GB/s; {c['sample']}")
