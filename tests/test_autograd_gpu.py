@@ -99,3 +99,25 @@ def test_matches_torch_gradient(gpu, dtype, rtol):
     assert torch.allclose(gB.double(), B64.grad, rtol=rtol, atol=rtol * float(B64.grad.abs().max()))
     del A, B, A64, B64
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_tsmm_accumulate_staged_and_unstaged_agree(gpu, dtype):
+    """Y += X W through the staged-Y kernel (dense Y: the old rows ride the
+    TMA ring) and through the unstaged one (Y a column slice of a wider
+    buffer: old pairs read from global memory) add the same product to the
+    same old values in the same order: bit-identical results."""
+    from tsm_benchmark_b200 import tsmm
+    for p, q in ((16, 16), (8, 64), (64, 4), (4, 32), (32, 32)):
+        for n in (5, 4099, 70001, (1 << 20) + 3):
+            g = torch.Generator().manual_seed(n + 7 * p + q)
+            X = torch.randn(n, p, generator=g, dtype=torch.float64).to(dtype).to(gpu)
+            W = torch.randn(p, q, generator=g, dtype=torch.float64).to(dtype).to(gpu)
+            Y0 = torch.randn(n, q, generator=g, dtype=torch.float64).to(dtype).to(gpu)
+            dense = Y0.clone()
+            wide = torch.zeros(n, q + 4, dtype=dtype, device=gpu)
+            wide[:, 2:2 + q] = Y0
+            tsmm(X, W, dense, accumulate=True)
+            tsmm(X, W, wide[:, 2:2 + q], accumulate=True)
+            assert torch.equal(dense, wide[:, 2:2 + q]), (p, q, n)
+            assert not torch.equal(dense, Y0), (p, q, n)

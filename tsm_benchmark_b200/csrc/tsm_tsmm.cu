@@ -44,6 +44,7 @@ constexpr int kTsmmCount = sizeof(kTsmm) / sizeof(kTsmm[0]);
 struct DmmaEntry {
   int dtype;  // 0 f64, 1 f32
   int P, Q;
+  bool ys;  // Y += X W with the old Y rows staged beside X (beta = 1, dense Y)
   const void* fn;
   int threads;
   size_t smem;
@@ -57,21 +58,45 @@ constexpr int dmma_rows() {
   return (sizeof(T) == 4 && P >= 16 ? 65536 : 32768) / (P * int(sizeof(T)));
 }
 
+// Staged-Y kernels (beta = 1, dense Y): stages of ~64 KB holding the X rows
+// and the old Y rows of a chunk; rows a power of two.
+template <typename T, int P, int Q>
+constexpr int dmma_ys_rows() {
+  int r = 1;
+  while (2 * r * (P + Q) * int(sizeof(T)) <= 65536) r *= 2;
+  return r;
+}
+
 #define TSM_DMMA_ENTRY(T, DT, P, Q)                                                                            \
   DmmaEntry {                                                                                                  \
-    DT, P, Q, reinterpret_cast<const void*>(&tsm_tsmm_dmma_kernel<T, P, Q, kCW, kStages, dmma_rows<T, P>()>),   \
+    DT, P, Q, false,                                                                                           \
+        reinterpret_cast<const void*>(&tsm_tsmm_dmma_kernel<T, P, Q, kCW, kStages, dmma_rows<T, P>()>),         \
         TsmmDmmaKernel<T, P, Q, kCW, kStages, dmma_rows<T, P>()>::THREADS,                                      \
         TsmmDmmaKernel<T, P, Q, kCW, kStages, dmma_rows<T, P>()>::SMEM_BYTES, dmma_rows<T, P>()                 \
+  }
+#define TSM_DMMA_YS_ENTRY(T, DT, P, Q)                                                                            \
+  DmmaEntry {                                                                                                     \
+    DT, P, Q, true,                                                                                               \
+        reinterpret_cast<const void*>(&tsm_tsmm_dmma_kernel<T, P, Q, kCW, kStages, dmma_ys_rows<T, P, Q>(), true>), \
+        TsmmDmmaKernel<T, P, Q, kCW, kStages, dmma_ys_rows<T, P, Q>(), true>::THREADS,                             \
+        TsmmDmmaKernel<T, P, Q, kCW, kStages, dmma_ys_rows<T, P, Q>(), true>::SMEM_BYTES,                          \
+        dmma_ys_rows<T, P, Q>()                                                                                   \
   }
 #define TSM_DMMA_ROW(T, DT, P)                                                                              \
   TSM_DMMA_ENTRY(T, DT, P, 4), TSM_DMMA_ENTRY(T, DT, P, 8), TSM_DMMA_ENTRY(T, DT, P, 16),                   \
       TSM_DMMA_ENTRY(T, DT, P, 32), TSM_DMMA_ENTRY(T, DT, P, 64)
+#define TSM_DMMA_YS_ROW(T, DT, P)                                                                           \
+  TSM_DMMA_YS_ENTRY(T, DT, P, 4), TSM_DMMA_YS_ENTRY(T, DT, P, 8), TSM_DMMA_YS_ENTRY(T, DT, P, 16),          \
+      TSM_DMMA_YS_ENTRY(T, DT, P, 32), TSM_DMMA_YS_ENTRY(T, DT, P, 64)
 
 const DmmaEntry kDmma[] = {
-    TSM_DMMA_ROW(double, 0, 4),  TSM_DMMA_ROW(double, 0, 8), TSM_DMMA_ROW(double, 0, 16),
-    TSM_DMMA_ROW(double, 0, 32), TSM_DMMA_ROW(double, 0, 64), TSM_DMMA_ROW(float, 1, 4),
-    TSM_DMMA_ROW(float, 1, 8),   TSM_DMMA_ROW(float, 1, 16),  TSM_DMMA_ROW(float, 1, 32),
-    TSM_DMMA_ROW(float, 1, 64),
+    TSM_DMMA_ROW(double, 0, 4),     TSM_DMMA_ROW(double, 0, 8),     TSM_DMMA_ROW(double, 0, 16),
+    TSM_DMMA_ROW(double, 0, 32),    TSM_DMMA_ROW(double, 0, 64),    TSM_DMMA_ROW(float, 1, 4),
+    TSM_DMMA_ROW(float, 1, 8),      TSM_DMMA_ROW(float, 1, 16),     TSM_DMMA_ROW(float, 1, 32),
+    TSM_DMMA_ROW(float, 1, 64),     TSM_DMMA_YS_ROW(double, 0, 4),  TSM_DMMA_YS_ROW(double, 0, 8),
+    TSM_DMMA_YS_ROW(double, 0, 16), TSM_DMMA_YS_ROW(double, 0, 32), TSM_DMMA_YS_ROW(double, 0, 64),
+    TSM_DMMA_YS_ROW(float, 1, 4),   TSM_DMMA_YS_ROW(float, 1, 8),   TSM_DMMA_YS_ROW(float, 1, 16),
+    TSM_DMMA_YS_ROW(float, 1, 32),  TSM_DMMA_YS_ROW(float, 1, 64),
 };
 constexpr int kDmmaCount = sizeof(kDmma) / sizeof(kDmma[0]);
 
@@ -122,11 +147,18 @@ void set_chunks(TsmmArgs<T>& a, int rows) {
   a.total_chunks = total;
 }
 
-int dmma_index(int dtype, int p, int q) {
+int dmma_index(int dtype, int p, int q, bool ys) {
   const int P = std::max(4, cap_of(p)), Q = std::max(4, cap_of(q));
   for (int i = 0; i < kDmmaCount; ++i)
-    if (kDmma[i].dtype == dtype && kDmma[i].P == P && kDmma[i].Q == Q) return i;
+    if (kDmma[i].dtype == dtype && kDmma[i].P == P && kDmma[i].Q == Q && kDmma[i].ys == ys) return i;
   return -1;
+}
+
+// Y += X W can stage the old Y rows through the ring when Y is dense (ldy =
+// q), 16-byte aligned and each row a multiple of 16 bytes.
+template <typename T>
+bool stages_y(const TsmmProblem<T>& pr) {
+  return pr.beta && pr.ldy == pr.q && (pr.q * sizeof(T)) % 16 == 0 && aligned16(pr.Y);
 }
 
 // Bulk path on the FP64 tensor cores: one launch when both problems share
@@ -136,8 +168,10 @@ template <typename T>
 tsm_status launch_dmma(cudaStream_t stream, int dev, int sms, const TsmmProblem<T>* probs, int nprob,
                        unsigned* error) {
   constexpr int dtype = sizeof(T) == 8 ? 0 : 1;
-  int idx[2] = {dmma_index(dtype, probs[0].p, probs[0].q),
-                nprob > 1 ? dmma_index(dtype, probs[1].p, probs[1].q) : -1};
+  bool ys = true;  // every problem of the launch stages its old Y rows
+  for (int i = 0; i < nprob; ++i) ys = ys && stages_y(probs[i]);
+  int idx[2] = {dmma_index(dtype, probs[0].p, probs[0].q, ys),
+                nprob > 1 ? dmma_index(dtype, probs[1].p, probs[1].q, ys) : -1};
   const bool together = nprob == 1 || idx[0] == idx[1];
   for (int l = 0; l < (together ? 1 : nprob); ++l) {
     const DmmaEntry& e = kDmma[idx[l]];

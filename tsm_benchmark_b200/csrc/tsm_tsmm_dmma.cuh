@@ -28,7 +28,14 @@
 //   * rows of X stream through the TMA ring exactly as in tsm_tsmm.cuh;
 //   * Y is stored from the D fragments: column pairs, streaming (evict-first)
 //     stores -- Y is not read again by this launch.
-// Each Y element is one FP64 sum in a fixed order: deterministic.
+//   * Y += X W (beta = 1) with YS = true: the producer streams each chunk's
+//     old Y rows into the same stage after its X rows (one more bulk copy,
+//     dense Y: ldy = q, q * sizeof(TX) a multiple of 16), and the consumers
+//     add them from shared memory.  Without YS, beta = 1 reads each old Y
+//     pair from global memory just before its store, one dependent load per
+//     pair, which leaves the read stream latency-bound.
+// Each Y element is one FP64 sum in a fixed order: deterministic (with beta,
+// the product's sum plus the old Y value, staged or not).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -40,7 +47,7 @@
 
 namespace tsm {
 
-template <typename TX, int P, int Q, int CW, int STAGES, int RS>
+template <typename TX, int P, int Q, int CW, int STAGES, int RS, bool YS = false>
 struct TsmmDmmaKernel {
   static_assert(P >= 4 && P <= 64 && (P & (P - 1)) == 0, "P: power of two in 4..64");
   static_assert(Q >= 4 && Q <= 64 && (Q & (Q - 1)) == 0, "Q: power of two in 4..64");
@@ -66,8 +73,10 @@ struct TsmmDmmaKernel {
   static constexpr int PASS = BLK * NRS;              // rows per CTA pass
   static_assert(RS % PASS == 0 && RS % 2 == 0, "chunk rows must be whole passes");
   static constexpr int THREADS = CW * 32 + 32;
-  static constexpr int STAGE = RS * P;  // elements per stage (capacity)
-  static constexpr size_t RING_BYTES = size_t(STAGES) * STAGE * sizeof(TX);
+  static constexpr int STAGE = RS * P;                // X elements per stage (capacity)
+  static constexpr int STAGE_ALL = STAGE + (YS ? RS * Q : 0);  // + old Y rows (YS)
+  static_assert((size_t(STAGE) * sizeof(TX)) % 16 == 0, "staged Y must start 16-byte aligned");
+  static constexpr size_t RING_BYTES = size_t(STAGES) * STAGE_ALL * sizeof(TX);
   static constexpr size_t BAR_OFFSET = (RING_BYTES + 127) / 128 * 128;
   static constexpr size_t SMEM_BYTES = BAR_OFFSET + 2 * STAGES * sizeof(uint64_t) + 16;
 };
@@ -124,12 +133,23 @@ __device__ __forceinline__ void store_pair(float* y, double v0, double v1, int b
   __stcs(reinterpret_cast<float2*>(y), make_float2(static_cast<float>(v0), static_cast<float>(v1)));
 }
 
+// Y += value with the old pair read from the staged rows in shared memory
+// (same sum as store_pair with beta: value + old, rounded once to TX).
+__device__ __forceinline__ void store_pair_staged(double* y, const double* old, double v0, double v1) {
+  const double2 o = *reinterpret_cast<const double2*>(old);
+  store_pair(y, v0 + o.x, v1 + o.y, 0);
+}
+__device__ __forceinline__ void store_pair_staged(float* y, const float* old, double v0, double v1) {
+  const float2 o = *reinterpret_cast<const float2*>(old);
+  store_pair(y, v0 + static_cast<double>(o.x), v1 + static_cast<double>(o.y), 0);
+}
+
 }  // namespace detail
 
-template <typename TX, int P, int Q, int CW, int STAGES, int RS>
-__global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>::THREADS, 1)
+template <typename TX, int P, int Q, int CW, int STAGES, int RS, bool YS = false>
+__global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS, YS>::THREADS, 1)
     tsm_tsmm_dmma_kernel(const TsmmArgs<TX> args) {
-  using K = TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>;
+  using K = TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS, YS>;
   extern __shared__ __align__(128) unsigned char smem[];
   TX* ring = reinterpret_cast<TX*>(smem);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + K::BAR_OFFSET);
@@ -165,8 +185,12 @@ __global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>::THRE
           const int64_t r0 = (c - (pi ? args.split : 0)) * RS;
           const int64_t rows = (pr.rows_main - r0) < RS ? (pr.rows_main - r0) : RS;
           const uint32_t bytes = static_cast<uint32_t>(rows * pr.p * sizeof(TX));
-          dev::mbar_arrive_expect_tx(&full[s], bytes);
-          dev::bulk_g2s_evict_first(ring + s * K::STAGE, pr.X + r0 * pr.p, bytes, &full[s], policy);
+          const uint32_t ybytes = YS ? static_cast<uint32_t>(rows * pr.q * sizeof(TX)) : 0u;
+          dev::mbar_arrive_expect_tx(&full[s], bytes + ybytes);
+          dev::bulk_g2s_evict_first(ring + s * K::STAGE_ALL, pr.X + r0 * pr.p, bytes, &full[s], policy);
+          if constexpr (YS)  // the old Y rows of the chunk (dense: pitch q)
+            dev::bulk_g2s_evict_first(ring + s * K::STAGE_ALL + K::STAGE, pr.Y + r0 * pr.q, ybytes, &full[s],
+                                      policy);
         } else {
           *abort = 1;
           atomicOr(args.error, dev::kErrTimeout);
@@ -199,14 +223,16 @@ __global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>::THRE
       }
       const int64_t r0 = (c - (pi ? args.split : 0)) * RS;
       const int rows = static_cast<int>((pr.rows_main - r0) < RS ? (pr.rows_main - r0) : RS);
-      const TX* stage = ring + s * K::STAGE;
+      const TX* stage = ring + s * K::STAGE_ALL;
+      const TX* ystage = stage + K::STAGE;  // old Y rows, pitch q (YS only)
       const int p = pr.p;
       const bool exact_p = p == P;
       const bool vec_y =
           pr.q == Q && (pr.ldy & 1) == 0 && (reinterpret_cast<uintptr_t>(pr.Y) & (2 * sizeof(TX) - 1)) == 0;
-      if (rows == RS && exact_p && vec_y && pr.ldy == Q && pr.beta == 0) {
-        // Fast path: a full chunk, p = P, q = Q = ldy, Y = X W.  Every
-        // stride is a compile-time constant and no row needs a guard.
+      if (rows == RS && exact_p && vec_y && pr.ldy == Q && (YS || pr.beta == 0)) {
+        // Fast path: a full chunk, p = P, q = Q = ldy, Y = X W (or, with YS,
+        // Y += X W from the staged rows).  Every stride is a compile-time
+        // constant and no row needs a guard.
         TX* const ybase = pr.Y + (r0 + g) * Q + o0 + 2 * t;
         const TX* const xbase = stage + g * P + (K::KPL == 2 ? 2 * t : t);
 #pragma unroll 1
@@ -238,8 +264,13 @@ __global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>::THRE
 #pragma unroll
             for (int i = 0; i < K::RG; ++i)
 #pragma unroll
-              for (int j = 0; j < K::NT; ++j)
-                detail::store_pair(ybase + (rb + 8 * i) * Q + 8 * j, d[i][j][0], d[i][j][1], 0);
+              for (int j = 0; j < K::NT; ++j) {
+                const int off = (rb + 8 * i + g) * Q + o0 + 8 * j + 2 * t;
+                if constexpr (YS)
+                  detail::store_pair_staged(ybase + (rb + 8 * i) * Q + 8 * j, ystage + off, d[i][j][0], d[i][j][1]);
+                else
+                  detail::store_pair(ybase + (rb + 8 * i) * Q + 8 * j, d[i][j][0], d[i][j][1], 0);
+              }
           }
         }
       } else
@@ -288,7 +319,16 @@ __global__ void __launch_bounds__(TsmmDmmaKernel<TX, P, Q, CW, STAGES, RS>::THRE
 #pragma unroll
           for (int j = 0; j < K::NT; ++j) {
             const int o = o0 + 8 * j + 2 * t;
-            if (vec_y) {
+            if constexpr (YS) {
+              // Dense Y (ldy = q): old values at r * q + o of the staged rows.
+              const TX* old = ystage + r * pr.q + o;
+              if (vec_y) {
+                if (Q >= 8 || o < Q) detail::store_pair_staged(yrow + o, old, d[i][j][0], d[i][j][1]);
+              } else {
+                if (o < pr.q) yrow[o] = static_cast<TX>(static_cast<double>(old[0]) + d[i][j][0]);
+                if (o + 1 < pr.q) yrow[o + 1] = static_cast<TX>(static_cast<double>(old[1]) + d[i][j][1]);
+              }
+            } else if (vec_y) {
               if (Q >= 8 || o < Q) detail::store_pair(yrow + o, d[i][j][0], d[i][j][1], pr.beta);
             } else {
               if (o < pr.q) detail::store_y(pr, r0 + r, o, static_cast<TX>(d[i][j][0]));
