@@ -242,16 +242,17 @@ namespace tsm {
 //
 // The 16-column blocks b of A give 8x8 tiles 2b (even columns) and 2b + 1
 // (odd columns).  Only block pairs (bi, bj) with bi <= bj are computed -- 4
-// tiles each, the lower tile of a diagonal pair included -- so C's upper
-// triangle is complete and the lower one is written by mirroring
+// tiles each off the diagonal, 3 on it (tile (1, 0) of a diagonal pair is
+// the transpose of tile (0, 1); gram_store writes it from that one) -- so
+// C's upper triangle is complete and the lower one is written by mirroring
 // (finish_partials with symmetric = 1).  Per k-step a warp loads each 16-column
 // block its region touches ONCE and feeds both DMMA operands from it (B is A).
-// Regions (lists of block pairs, equal tile counts, <= 20 tiles):
+// Regions (lists of block pairs, DMMA tiles per k-step, <= 20 per region):
 //   W = 16: {(0,0)}                                         1 region
-//   W = 32: {(0,0),(0,1),(1,1)}                             1 region, 12 of 16 tiles
-//   W = 48: {(0,0),(0,1),(1,1)}, {(0,2),(1,2),(2,2)}        24 of 36 tiles
+//   W = 32: {(0,0),(0,1),(1,1)}                             1 region, 10 of 16 tiles
+//   W = 48: {(0,0),(0,1),(1,1)}, {(0,2),(1,2),(2,2)}        21 of 36 tiles
 //   W = 64: {(0,0),(0,1),(0,2),(0,3),(1,1)},
-//           {(1,2),(1,3),(2,2),(2,3),(3,3)}                 40 of 64 tiles
+//           {(1,2),(1,3),(2,2),(2,3),(3,3)}                 36 of 64 tiles
 // A pair is coded 4 bi + bj, four bits per pair.
 __host__ __device__ constexpr int gram_regions(int W) { return W >= 48 ? 2 : 1; }
 __host__ __device__ constexpr int gram_npairs(int W, int) { return W == 16 ? 1 : (W == 64 ? 5 : 3); }
@@ -342,7 +343,10 @@ __device__ __forceinline__ void gram_consume(const PlainArgs<double>& p, unsigne
 #pragma unroll
         for (int a = 0; a < 2; ++a)
 #pragma unroll
-          for (int b = 0; b < 2; ++b) dev::dmma_m8n8k4(out[q][a][b][0], out[q][a][b][1], v[bi][a], v[bj][b]);
+          for (int b = 0; b < 2; ++b) {
+            if (bi == bj && a == 1 && b == 0) continue;  // the transpose of tile (0, 1): stored from it
+            dev::dmma_m8n8k4(out[q][a][b][0], out[q][a][b][1], v[bi][a], v[bj][b]);
+          }
       }
     }
     __syncwarp();
@@ -351,7 +355,13 @@ __device__ __forceinline__ void gram_consume(const PlainArgs<double>& p, unsigne
 }
 
 // Tile (pair q, parities a, b) -> C row 16 bi + 2 g + a, column 16 bj + 2 n + b
-// for D column n = 2 tq + e.
+// for D column n = 2 tq + e.  On a diagonal pair (bi = bj), tile (1, 0) is
+// the transpose of tile (0, 1) -- entry (g, n) of one is entry (n, g) of the
+// other, the same products summed over the same rows -- so the consumer
+// skips its DMMAs and tile (0, 1) is stored a second time, transposed, in
+// its place.  That brings the tiles per k-step to the upper triangle of the
+// 8 x 8 tiles: 3 of 4 at W = 16, 10 of 16 at 32, 21 of 36 at 48, 36 of 64 at
+// 64 (12, 24 and 40 before).
 template <int W, int REG>
 __device__ __forceinline__ void gram_store(double* sheet, int lane, const double (&out)[kGramMaxPairs][2][2][2]) {
   constexpr int NP = gram_npairs(W, REG);
@@ -364,8 +374,12 @@ __device__ __forceinline__ void gram_store(double* sheet, int lane, const double
 #pragma unroll
       for (int b = 0; b < 2; ++b)
 #pragma unroll
-        for (int e = 0; e < 2; ++e)
-          sheet[(16 * bi + 2 * g + a) * W + 16 * bj + 2 * (2 * tq + e) + b] = out[q][a][b][e];
+        for (int e = 0; e < 2; ++e) {
+          if (bi == bj && a == 1 && b == 0)  // C[16 bi + 2 n + 1][16 bi + 2 g] = tile (0, 1) entry (g, n)
+            sheet[(16 * bi + 2 * (2 * tq + e) + 1) * W + 16 * bi + 2 * g] = out[q][0][1][e];
+          else
+            sheet[(16 * bi + 2 * g + a) * W + 16 * bj + 2 * (2 * tq + e) + b] = out[q][a][b][e];
+        }
   }
 }
 
