@@ -141,3 +141,19 @@ def test_gram_candidates():
              "wa": v.wa, "wb": v.wb} for v in codegen.default_variants()]
     for w in GRAM_WIDTHS:
         assert gram_candidates(real, w), w
+
+
+def test_dmma_chunk_rows_rule():
+    """DMMA chunks of more than 256 rows are split into equal tensor boxes of
+    at most 256 rows, each a whole number of 8-row swizzle groups (the kernel's
+    dmma_rows_ok); other row counts are rejected by the generator."""
+    from tsm_benchmark_b200.codegen import DmmaVariant
+    ok = [DmmaVariant(16, 16, rows=384, stages=2), DmmaVariant(16, 16, rows=288, stages=3),
+          DmmaVariant(16, 16, rows=768, stages=2, gram=True), DmmaVariant(32, 32, rows=192, stages=2)]
+    for v in ok:
+        assert v.validate() == [], v.name
+    bad = [DmmaVariant(16, 16, rows=264, stages=2),   # two boxes of 132 rows: not whole 8-row groups
+           DmmaVariant(16, 16, rows=300, stages=2),   # not a multiple of 8
+           DmmaVariant(16, 16, rows=1032, stages=1)]  # above 1024
+    for v in bad:
+        assert any("chunk rows" in e for e in v.validate()), v.rows
