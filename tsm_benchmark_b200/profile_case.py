@@ -3,7 +3,7 @@
 under a profiler (ncu) or to time one variant.
 
     python -m tsm_benchmark_b200.profile_case --n 4194304 --m 8 --k 8 --reps 4 [--variant NAME]
-    python -m tsm_benchmark_b200.profile_case --form split|backward|gram|batched --n ... --m ... --k ...
+    python -m tsm_benchmark_b200.profile_case --form split|backward|gram|batched|block_orth --n ... --m ... --k ...
     python -m tsm_benchmark_b200.profile_case --layout col --n ... --m ... --k ...   (A^T, B^T row-major)
 
 One untimed call comes first (library setup); a profiler capture of the k-th
@@ -29,9 +29,11 @@ def main(argv=None) -> int:
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--reps", type=int, default=4)
     ap.add_argument("--variant", default=None, help="variant name (default: the library's choice)")
-    ap.add_argument("--form", choices=["plain", "split", "backward", "gram", "batched"], default="plain",
+    ap.add_argument("--form", choices=["plain", "split", "backward", "gram", "batched", "block_orth"],
+                    default="plain",
                     help="plain FP64, FP32 TF32-split on tensor cores, the fused backward, the Gram product "
-                         "C = A^T A, or a batch of --count products of n rows and widths m x k in one launch")
+                         "C = A^T A, a batch of --count products of n rows and widths m x k in one launch, or "
+                         "block orthogonalisation B <- B - A (A^T B) (two launches: the product, then the TSMM)")
     ap.add_argument("--count", type=int, default=64, help="problems in the batch (--form batched)")
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64", help="storage type of the backward")
     ap.add_argument("--split-kind", choices=["tf32", "bf16x2", "bf16x3"], default="tf32",
@@ -41,15 +43,25 @@ def main(argv=None) -> int:
                          "through tsm_gemm_tn_strided_f64)")
     args = ap.parse_args(argv)
 
-    from tsm_benchmark_b200 import (BatchedTSMTTSM, fill_uniform, gram, tsmttsm, tsmttsm_backward, tsmttsm_split,
-                                    variants)
+    from tsm_benchmark_b200 import (BatchedTSMTTSM, block_orthogonalize, fill_uniform, gram, tsmttsm,
+                                    tsmttsm_backward, tsmttsm_split, variants)
     dev = torch.device("cuda", 0)
-    if args.form in ("gram", "batched"):
+    if args.form in ("gram", "batched", "block_orth"):
         if args.form == "gram":
             A = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
             fill_uniform(A, 1, 0)
             run = lambda: gram(A)  # noqa: E731
             nbytes = 8 * args.n * args.m
+        elif args.form == "block_orth":
+            # A's columns scaled to about unit norm, so repeated steps keep B bounded.
+            A = torch.empty((args.n, args.m), dtype=torch.float64, device=dev)
+            B = torch.empty((args.n, args.k), dtype=torch.float64, device=dev)
+            fill_uniform(A, 1, 0)
+            fill_uniform(B, 1, 1)
+            A.mul_(math.sqrt(3.0 / max(args.n, 1)))
+            C = torch.empty((args.m, args.k), dtype=torch.float64, device=dev)
+            run = lambda: block_orthogonalize(A, B, C)  # noqa: E731
+            nbytes = 8 * args.n * (2 * args.m + 3 * args.k)  # A and B read twice, B written once
         else:
             As, Bs = [], []
             for i in range(args.count):
