@@ -200,8 +200,15 @@ def test_generated_kernels_name_compiled_variants():
     kinds = [codegen.pick_dropin_variant(vs, 8, 4, lf, sg)[0] for lf, sg in
              ((False, False), (True, False), (False, True), (True, True))]
     assert kinds[2] is None and len({kinds[0], kinds[1], kinds[3]}) == 3
-    # widths 16..64: the prefetching reduction-optimised name runs the FP64 tensor cores
+    # widths 16..64: the prefetching reduction-optimised name runs the FP64 tensor cores, on a
+    # kernel that is not one of the tuned choices the plain reduction-optimised name runs
+    tuned = codegen.load_tuned()
     for m in (16, 32, 64):
-        assert codegen.pick_dropin_variant(vs, m, 4, True, True)[0].startswith("dmma_")
+        name = codegen.pick_dropin_variant(vs, m, 4, True, True)[0]
+        assert name.startswith("dmma_")
+        assert name not in {t[3] for t in tuned if (t[0], t[1]) == (m, m)} or \
+            len([v for v in vs if isinstance(v, codegen.DmmaVariant) and not v.gram and (v.wa, v.wb) == (m, m)]) == 1
+    fake = [(16, 16, 0, "dmma_16x16_t16x16_w8_s2_r384")]
+    assert codegen.pick_dropin_variant(vs, 16, 4, True, True, tuned=fake)[0] == "dmma_16x16_t16x16_w8_s3_r288"
     # the CTA cap is stride / local_size work-groups
     assert "K, 8, 8, A, B, C, variant, 2048);" in codegen.render_dropin_header(vs, widths=(8,), tiles=(4,))

@@ -570,7 +570,7 @@ def _covers(v, m: int) -> bool:
 
 
 def pick_dropin_variant(vs: list, m: int, tm: int, prefetch: bool, reduce_opt: bool, local_size: int = 256,
-                        unroll: int = 1) -> tuple[str | None, str]:
+                        unroll: int = 1, tuned: list | None = None) -> tuple[str | None, str]:
     """The compiled FP64 variant a generated drop-in kernel runs, and why.
 
     The reference's options map onto this library's axes as follows:
@@ -580,8 +580,9 @@ def pick_dropin_variant(vs: list, m: int, tm: int, prefetch: bool, reduce_opt: b
         shallowest (a double buffer of long copies, the leap-frog's analogue);
       * the reduction-optimised kernels (_sg / _2l) -> the autotuned choice
         for (M, M, K) (FP64 tensor cores for widths 16..64), and with _lf the
-        tensor-core kernel's shallowest ring, or the SIMT tile's middle ring
-        below width 16;
+        tensor-core kernel's shallowest ring that is not one of the tuned
+        choices for (M, M) (so the two names time different kernels), or
+        the SIMT tile's middle ring below width 16;
       * local_size -> consumer warps (local_size / 32) and --unroll -> the
         row-loop unroll, where such a variant is compiled.
     None means the library's autotuned default at run time."""
@@ -592,8 +593,14 @@ def pick_dropin_variant(vs: list, m: int, tm: int, prefetch: bool, reduce_opt: b
     if reduce_opt and prefetch:
         dm = [v.resolved() for v in vs if isinstance(v, DmmaVariant) and not v.gram and (v.wa, v.wb) == (m, m)]
         if dm:
-            v = min(dm, key=lambda d: (d.stages, -d.rows))
-            return v.name if isinstance(v, DmmaVariant) else None, "FP64 tensor cores, shallowest ring"
+            tuned_names = {name for tm_, tk_, _, name in (load_tuned() if tuned is None else tuned)
+                           if (tm_, tk_) == (m, m)}
+            order = sorted(dm, key=lambda d: (d.stages, -d.rows))
+            v = next((d for d in order if d.name not in tuned_names), order[0])
+            why = "FP64 tensor cores, shallowest ring"
+            if v is not order[0]:
+                why += " other than the autotuned choice"
+            return v.name, why
     if not simt:
         return None, "no SIMT tile compiled for this width: the autotuned default"
     exact = [v for v in simt if v.exact]
