@@ -53,13 +53,16 @@ constexpr int cm_simt_rs(int wa, int wb) {
                                   : std::max(64, 12288 / (wa + wb) / 32 * 32);
 }
 constexpr int kCmSimtStages = 2;
-// DMMA: regions of at most 4 x 4 tiles, 8 consumer warps, ~64 KB chunks of
-// whole 16-value groups (boxes of RS + 2 <= 256 values), as many stages as
-// fit 220 KB (2 to 4).
+// DMMA: regions of at most 4 x 4 tiles, 8 consumer warps, chunks of whole
+// 16-value groups sized for two ~98 KB stages (boxes of RS + 2 <= 242
+// values), as many stages as fit 220 KB (2 to 4).  Against ~64 KB chunks
+// (three interleaved rounds, one B200): 32 x 32 at 2^25 7143-7159 vs
+// 6894-6944 GB/s, 32 x 64 at 2^24 6227-6282 vs 5957-6038, 64 x 64 at 2^23
+// 4186-4210 vs 4148-4169; 16 x 16 and narrower keep their 240-value chunks.
 constexpr int cm_tiles(int w) {
   return (w / 8) % 4 == 0 ? 4 : (w / 8) % 3 == 0 ? 3 : (w / 8) % 2 == 0 ? 2 : 1;
 }
-constexpr int cm_dmma_rs(int wa, int wb) { return std::min(240, std::max(16, (8192 / (wa + wb) - 2) / 16 * 16)); }
+constexpr int cm_dmma_rs(int wa, int wb) { return std::min(240, std::max(16, (12544 / (wa + wb) - 2) / 16 * 16)); }
 constexpr int cm_dmma_stages(int wa, int wb) {
   return std::max(2, std::min(4, (220 * 1024) / ((wa + wb) * 8 * (cm_dmma_rs(wa, wb) + 2))));
 }
