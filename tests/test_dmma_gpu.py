@@ -57,13 +57,15 @@ def test_dmma_strided_operands(gpu, oracle_mod):
 
 def test_dmma_repeatable(gpu, oracle_mod):
     from tsm_benchmark_b200 import tsmttsm
-    (v,) = [v for v in dmma_variants() if (v["wa"], v["wb"]) == (64, 64)]
+    vs = [v for v in dmma_variants() if (v["wa"], v["wb"]) == (64, 64)]  # every ring shape
+    assert vs
     A, B = oracle_mod.operands(300007, 64, 64, 9)
     dA, dB = to_dev(A, gpu), to_dev(B, gpu)
-    C1 = tsmttsm(dA, dB, variant=v["index"])
-    C2 = tsmttsm(dA, dB, variant=v["index"])
-    assert torch.equal(C1, C2)
-    assert_parity(oracle_mod, A, B, C1, what="dmma 64x64 large")
+    for v in vs:
+        C1 = tsmttsm(dA, dB, variant=v["index"])
+        C2 = tsmttsm(dA, dB, variant=v["index"])
+        assert torch.equal(C1, C2), v["name"]
+        assert_parity(oracle_mod, A, B, C1, what=f"{v['name']} large")
 
 
 def test_dmma_accumulate(gpu, oracle_mod):

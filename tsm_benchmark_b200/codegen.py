@@ -413,6 +413,8 @@ def default_variants() -> list:
         out.append(DmmaVariant(16, 16, rows=rows, stages=stages))
     for rows, stages in ((768, 2), (512, 3)):
         out.append(DmmaVariant(16, 16, rows=rows, stages=stages, gram=True))
+    # 64 x 64 (FP64-bound) on 2 x 96 KB as well as 3 x 64 KB.
+    out.append(DmmaVariant(64, 64, rows=96, stages=2))
     # The wider Gram kernels (FP64- and HBM-bound at once) with 2 x 96 KB rings;
     # width 32 also with 12 consumer warps.
     for w, rows, cw in ((32, 384, 8), (32, 384, 12), (48, 256, 0), (64, 192, 0)):
@@ -600,6 +602,8 @@ def pick_dropin_variant(vs: list, m: int, tm: int, prefetch: bool, reduce_opt: b
             why = "FP64 tensor cores, shallowest ring"
             if v is not order[0]:
                 why += " other than the autotuned choice"
+            elif v.name in tuned_names:
+                why += " (an autotuned choice too: every ring compiled for this width is one for some row count)"
             return v.name, why
     if not simt:
         return None, "no SIMT tile compiled for this width: the autotuned default"
