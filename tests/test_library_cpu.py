@@ -206,8 +206,9 @@ def test_generated_kernels_name_compiled_variants():
     for m in (16, 32, 64):
         name = codegen.pick_dropin_variant(vs, m, 4, True, True)[0]
         assert name.startswith("dmma_")
-        assert name not in {t[3] for t in tuned if (t[0], t[1]) == (m, m)} or \
-            len([v for v in vs if isinstance(v, codegen.DmmaVariant) and not v.gram and (v.wa, v.wb) == (m, m)]) == 1
+        tuned_m = {t[3] for t in tuned if (t[0], t[1]) == (m, m)}
+        rings = {v.name for v in vs if isinstance(v, codegen.DmmaVariant) and not v.gram and (v.wa, v.wb) == (m, m)}
+        assert name not in tuned_m or rings <= tuned_m  # else every compiled ring is a tuned choice
     fake = [(16, 16, 0, "dmma_16x16_t16x16_w8_s2_r384")]
     assert codegen.pick_dropin_variant(vs, 16, 4, True, True, tuned=fake)[0] == "dmma_16x16_t16x16_w8_s3_r288"
     # the CTA cap is stride / local_size work-groups
