@@ -179,7 +179,9 @@ def reference_cpu(n_sample: int, steps: int, warmup: int, budget_s: float) -> di
         naive = {"value": algo_bytes(nn, HEAD_M, HEAD_K) / tn / 1e9, "unit": "GB/s", "cores": 1,
                  "sample": f"compute_naive, n={nn} rows x m=k=8, one run of {tn * 1e3:.1f} ms"}
     return {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind, "steps_timed": len(times),
-            "sample": (f"n={n_sample} rows x m=k=8 (the headline shape at {n_sample / HEAD_N:.4g} of its rows), "
+            "sample": (f"n={n_sample} rows x m=k=8 ("
+                       + ("the headline shape, all of its rows" if n_sample == HEAD_N
+                          else f"the headline shape at {n_sample / HEAD_N:.4g} of its rows") + "), "
                        f"tsmttsm4 stride {REF_STRIDE} tile {REF_TILE}, mean of {len(times)} runs "
                        f"of {t * 1e3:.1f} ms"),
             "naive_single_core": naive}
