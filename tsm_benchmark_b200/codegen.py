@@ -415,6 +415,10 @@ def default_variants() -> list:
         out.append(DmmaVariant(16, 16, rows=rows, stages=stages, gram=True))
     # 64 x 64 (FP64-bound) on 2 x 96 KB as well as 3 x 64 KB.
     out.append(DmmaVariant(64, 64, rows=96, stages=2))
+    # More consumer warps on the 2 x 96 KB rings (the Gram kernel of width 32
+    # gained from 12): 32 x 32, 16 x 16 and 64 x 64 with 12.
+    for w, rows, cw in ((32, 192, 12), (16, 384, 12), (64, 96, 12)):
+        out.append(DmmaVariant(w, w, rows=rows, stages=2, cw=cw))
     # The wider Gram kernels (FP64- and HBM-bound at once) with 2 x 96 KB rings;
     # width 32 also with 12 consumer warps.
     for w, rows, cw in ((32, 384, 8), (32, 384, 12), (48, 256, 0), (64, 192, 0)):

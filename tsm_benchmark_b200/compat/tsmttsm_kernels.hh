@@ -161,10 +161,10 @@ sycl::event tsmttsm_16_16_2_2_sg(sycl::queue& q, int K, const T* A, const T* B, 
   return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant, 2048);
 }
 
-// runs dmma_16x16_t16x16_w8_s3_r288: FP64 tensor cores, shallowest ring other than the autotuned choice
+// runs dmma_16x16_t16x16_w12_s2_r384: FP64 tensor cores, shallowest ring other than the autotuned choice
 template <typename T>
 sycl::event tsmttsm_16_16_2_2_sg_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
-  static const int variant = tsm_compat::variant_by_name("dmma_16x16_t16x16_w8_s3_r288");
+  static const int variant = tsm_compat::variant_by_name("dmma_16x16_t16x16_w12_s2_r384");
   return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant, 2048);
 }
 
@@ -189,10 +189,10 @@ sycl::event tsmttsm_16_16_4_4_sg(sycl::queue& q, int K, const T* A, const T* B, 
   return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant, 2048);
 }
 
-// runs dmma_16x16_t16x16_w8_s3_r288: FP64 tensor cores, shallowest ring other than the autotuned choice
+// runs dmma_16x16_t16x16_w12_s2_r384: FP64 tensor cores, shallowest ring other than the autotuned choice
 template <typename T>
 sycl::event tsmttsm_16_16_4_4_sg_lf(sycl::queue& q, int K, const T* A, const T* B, T* C) {
-  static const int variant = tsm_compat::variant_by_name("dmma_16x16_t16x16_w8_s3_r288");
+  static const int variant = tsm_compat::variant_by_name("dmma_16x16_t16x16_w12_s2_r384");
   return tsm_compat::accumulate_tn<T>(q, K, 16, 16, A, B, C, variant, 2048);
 }
 

@@ -52,7 +52,7 @@ const Variant kGenPart0[] = {
     TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s2_r6144_u1_gram", double, 2, 2, 2, 2, 8, 2, 6144, 1, true, true),
     TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s6_r2048_u1_gram", double, 2, 2, 2, 2, 8, 6, 2048, 1, true, true),
     TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s2_r384", 16, 16, 2, 2, 8, 2, 384),
-    TSM_GRAM_DMMA_VARIANT("dmma_64x64_gram_w8_s2_r192", 64, 8, 2, 192),
+    TSM_GRAM_DMMA_VARIANT("dmma_32x32_gram_w8_s2_r384", 32, 8, 2, 384),
 };
 extern const int kGenPart0Count;
 const int kGenPart0Count = 46;

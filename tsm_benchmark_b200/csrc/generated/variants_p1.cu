@@ -52,8 +52,9 @@ const Variant kGenPart1[] = {
     TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s2_r3072_u1_gram", double, 4, 4, 4, 4, 8, 2, 3072, 1, true, true),
     TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s6_r1024_u1_gram", double, 4, 4, 4, 4, 8, 6, 1024, 1, true, true),
     TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s3_r288", 16, 16, 2, 2, 8, 3, 288),
+    TSM_GRAM_DMMA_VARIANT("dmma_32x32_gram_w12_s2_r384", 32, 12, 2, 384),
 };
 extern const int kGenPart1Count;
-const int kGenPart1Count = 45;
+const int kGenPart1Count = 46;
 
 }  // namespace tsm

@@ -52,8 +52,9 @@ const Variant kGenPart2[] = {
     TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s2_r1536_u1_gram", double, 8, 8, 4, 4, 8, 2, 1536, 1, true, true),
     TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s6_r512_u1_gram", double, 8, 8, 4, 4, 8, 6, 512, 1, true, true),
     TSM_GRAM_DMMA_VARIANT("dmma_16x16_gram_w8_s2_r768", 16, 8, 2, 768),
+    TSM_GRAM_DMMA_VARIANT("dmma_48x48_gram_w8_s2_r256", 48, 8, 2, 256),
 };
 extern const int kGenPart2Count;
-const int kGenPart2Count = 45;
+const int kGenPart2Count = 46;
 
 }  // namespace tsm

@@ -52,8 +52,9 @@ const Variant kGenPart3[] = {
     TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s3_r8192_u1_gram", double, 1, 1, 1, 1, 8, 3, 8192, 1, true, true),
     TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s4_r192", 16, 16, 2, 2, 8, 4, 192),
     TSM_GRAM_DMMA_VARIANT("dmma_16x16_gram_w8_s3_r512", 16, 8, 3, 512),
+    TSM_GRAM_DMMA_VARIANT("dmma_64x64_gram_w8_s2_r192", 64, 8, 2, 192),
 };
 extern const int kGenPart3Count;
-const int kGenPart3Count = 45;
+const int kGenPart3Count = 46;
 
 }  // namespace tsm

@@ -51,7 +51,7 @@ const Variant kGenPart6[] = {
     TSM_GRAM_DMMA_VARIANT("dmma_64x64_gram_w8_s3_r128", 64, 8, 3, 128),
     TSM_BULK_VARIANT("bulk_8x8_t4x4_w8_s3_r1024_u1_gram", double, 8, 8, 4, 4, 8, 3, 1024, 1, true, true),
     TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s2_r192", 32, 32, 4, 4, 8, 2, 192),
-    TSM_GRAM_DMMA_VARIANT("dmma_32x32_gram_w12_s2_r384", 32, 12, 2, 384),
+    TSM_DMMA_VARIANT("dmma_16x16_t16x16_w12_s2_r384", 16, 16, 2, 2, 12, 2, 384),
 };
 extern const int kGenPart6Count;
 const int kGenPart6Count = 45;

@@ -51,7 +51,7 @@ const Variant kGenPart7[] = {
     TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s2_r12288_u1_gram", double, 1, 1, 1, 1, 8, 2, 12288, 1, true, true),
     TSM_BULK_VARIANT("bulk_1x1_t1x1_w8_s6_r4096_u1_gram", double, 1, 1, 1, 1, 8, 6, 4096, 1, true, true),
     TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s6_r64", 32, 32, 4, 4, 8, 6, 64),
-    TSM_GRAM_DMMA_VARIANT("dmma_48x48_gram_w8_s2_r256", 48, 8, 2, 256),
+    TSM_DMMA_VARIANT("dmma_64x64_t32x32_w12_s2_r96", 64, 64, 4, 4, 12, 2, 96),
 };
 extern const int kGenPart7Count;
 const int kGenPart7Count = 45;
