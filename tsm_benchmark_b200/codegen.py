@@ -421,7 +421,7 @@ def default_variants() -> list:
         out.append(DmmaVariant(w, w, rows=rows, stages=2, cw=cw))
     # The wider Gram kernels (FP64- and HBM-bound at once) with 2 x 96 KB rings;
     # width 32 also with 12 consumer warps.
-    for w, rows, cw in ((32, 384, 8), (32, 384, 12), (48, 256, 0), (64, 192, 0)):
+    for w, rows, cw in ((32, 384, 8), (32, 384, 12), (48, 256, 0), (64, 192, 0), (48, 240, 12), (64, 192, 12)):
         out.append(DmmaVariant(w, w, rows=rows, stages=2, cw=cw, gram=True))
     return out
 

@@ -52,8 +52,9 @@ const Variant kGenPart4[] = {
     TSM_BULK_VARIANT("bulk_2x2_t2x2_w8_s3_r4096_u1_gram", double, 2, 2, 2, 2, 8, 3, 4096, 1, true, true),
     TSM_DMMA_VARIANT("dmma_16x16_t16x16_w8_s6_r128", 16, 16, 2, 2, 8, 6, 128),
     TSM_DMMA_VARIANT("dmma_64x64_t32x32_w8_s2_r96", 64, 64, 4, 4, 8, 2, 96),
+    TSM_GRAM_DMMA_VARIANT("dmma_48x48_gram_w12_s2_r240", 48, 12, 2, 240),
 };
 extern const int kGenPart4Count;
-const int kGenPart4Count = 45;
+const int kGenPart4Count = 46;
 
 }  // namespace tsm

@@ -52,8 +52,9 @@ const Variant kGenPart5[] = {
     TSM_BULK_VARIANT("bulk_4x4_t4x4_w8_s3_r2048_u1_gram", double, 4, 4, 4, 4, 8, 3, 2048, 1, true, true),
     TSM_DMMA_VARIANT("dmma_32x32_t32x32_w8_s4_r96", 32, 32, 4, 4, 8, 4, 96),
     TSM_DMMA_VARIANT("dmma_32x32_t32x32_w12_s2_r192", 32, 32, 4, 4, 12, 2, 192),
+    TSM_GRAM_DMMA_VARIANT("dmma_64x64_gram_w12_s2_r192", 64, 12, 2, 192),
 };
 extern const int kGenPart5Count;
-const int kGenPart5Count = 45;
+const int kGenPart5Count = 46;
 
 }  // namespace tsm
