@@ -157,3 +157,22 @@ def test_dmma_chunk_rows_rule():
            DmmaVariant(16, 16, rows=1032, stages=1)]  # above 1024
     for v in bad:
         assert any("chunk rows" in e for e in v.validate()), v.rows
+
+
+def test_modes_keep_each_others_sections():
+    """A plain tuning rewrites choices and timings and keeps the batched paths
+    and the Gram table of the file it replaces; merging one pair keeps the
+    other pairs' choices."""
+    from tsm_benchmark_b200.autotune import keep_sections, merge_results
+    old = {"choices": [{"m": 8, "k": 8, "nmin": 0, "variant": "a"}, {"m": 16, "k": 16, "nmin": 0, "variant": "b"}],
+           "timings": {"8x8@1": {}, "16x16@1": {}},
+           "batched_paths": [{"m": 16, "k": 16, "path": "dmma"}],
+           "gram_choices": [{"w": 16, "nmin": 0, "variant": "g"}], "gram_timings": {"gram16@1": {}}}
+    res = {"choices": [{"m": 16, "k": 16, "nmin": 0, "variant": "c"}], "timings": {"16x16@1": {"x": 1}}}
+    merged = keep_sections(merge_results(old, res, [(16, 16)]), old)
+    assert [(c["m"], c["variant"]) for c in merged["choices"]] == [(8, "a"), (16, "c")]
+    assert merged["timings"]["16x16@1"] == {"x": 1} and "8x8@1" in merged["timings"]
+    for key in ("batched_paths", "gram_choices", "gram_timings"):
+        assert merged[key] == old[key], key
+    # a section the new result carries is not overwritten by the old one
+    assert keep_sections({"gram_choices": []}, old)["gram_choices"] == []

@@ -92,6 +92,16 @@ def median_winner(samples: dict) -> tuple[str, dict]:
     return min(med, key=med.get), med
 
 
+def keep_sections(res: dict, old: dict) -> dict:
+    """`res` with the sections of an earlier file `old` that this mode did not
+    write (KEPT_SECTIONS: another mode's tuning) carried over."""
+    out = dict(res)
+    for key in KEPT_SECTIONS:
+        if key not in out and key in old:
+            out[key] = old[key]
+    return out
+
+
 def merge_results(old: dict, res: dict, pairs) -> dict:
     """`res` (a tuning of `pairs`) with the other pairs' choices and timings
     of an earlier result `old` kept; choices sorted by (m, k, nmin)."""
@@ -334,10 +344,7 @@ def main(argv=None) -> int:
             res = merge_results(json.load(f), res, pairs)
     if os.path.exists(args.out):
         with open(args.out) as f:
-            old = json.load(f)
-        for key in KEPT_SECTIONS:
-            if key not in res and key in old:
-                res[key] = old[key]
+            res = keep_sections(res, json.load(f))
     with open(args.out, "w") as f:
         json.dump(res, f, indent=1)
         f.write("\n")
